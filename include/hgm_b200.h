@@ -1,0 +1,150 @@
+/*
+ * hgm_b200.h -- native C-ABI of the B200 state-vector engine (libhgm_b200.so).
+ *
+ * Plain pointers and sizes only.  Every function returns an int status
+ * (HGM_OK == 0) unless noted; hgm_last_error() gives the message of the
+ * last failure on the calling thread.
+ *
+ * Conventions shared with the reference (MMullerdR/simulador_quantico):
+ *   - a state of n qubits is 2^n interleaved complex amplitudes (re, im);
+ *     index bit b belongs to circuit qubit n-1-b
+ *     (docs/01-arquitetura-geral.md, src/core/dgm_core.cpp:72);
+ *   - an op is a controlled 1-qubit gate: target index bit, control mask and
+ *     value (applied iff (index & mask) == value) and a row-major 2x2 complex
+ *     matrix [m00, m01, m10, m11] given as 8 doubles (re, im)
+ *     (struct PT, include/core/common.h:57-90; src/core/kernel.cu:109-111).
+ *
+ * Precision: HGM_F64 states hold complex128, HGM_F32 complex64 (gate
+ * matrices are always built in FP64 and cast).
+ */
+#ifndef HGM_B200_H
+#define HGM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HGM_OK 0
+#define HGM_ERR_INVALID 1      /* bad argument / malformed circuit */
+#define HGM_ERR_CUDA 2         /* CUDA runtime error */
+#define HGM_ERR_NOMEM 3        /* device allocation failed / over budget */
+#define HGM_ERR_UNSUPPORTED 4  /* feature or size not provided */
+#define HGM_ERR_TIMEOUT 5      /* a bounded device wait gave up */
+#define HGM_ERR_BUSY 6         /* admission refused (serving) */
+
+#define HGM_F64 0
+#define HGM_F32 1
+
+typedef struct hgm_circuit hgm_circuit;
+typedef struct hgm_plan hgm_plan;
+typedef struct hgm_state hgm_state;
+
+/* ---- runtime ---------------------------------------------------------- */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *hgm_last_error(void);
+/* Initialises the CUDA context on `device` (setDevice, src/core/kernel.cu:31-33). */
+int hgm_init(int device);
+/* Blocks until all work queued by this library has finished. */
+int hgm_synchronize(void);
+/* Free / total device memory in bytes. */
+int hgm_mem_info(int64_t *free_bytes, int64_t *total_bytes);
+/* Number of kernel launches issued by this library since load. */
+int64_t hgm_kernel_launches(void);
+
+/* ---- circuits: host mirror of the DGM circuit language ------------------ */
+/* The circuit language of docs/02-linguagem-de-circuitos.md: steps separated
+ * by ';', one token per qubit separated by ','; tokens ID, a gate name,
+ * ControlN(v), TargetN(gate).  Parsed exactly as DGM::setFunction /
+ * genGroups / genPTs (src/core/dgm_parser.cpp:29-169). */
+
+hgm_circuit *hgm_circuit_new(void);
+void hgm_circuit_free(hgm_circuit *c);
+/* Gates::addGate (src/core/gates.cpp:42-60): registers a 2x2 matrix under
+ * `name`; returns 1 if added, 0 if the name already exists (never
+ * overwrites), <0 on error. */
+int hgm_circuit_add_gate(hgm_circuit *c, const char *name, const double m[8]);
+/* DGM::setFunction(string, iterations, reset) (dgm_parser.cpp:29-66). */
+int hgm_circuit_set_function(hgm_circuit *c, const char *steps, int iterations, int reset);
+/* Appends one op directly (no string). */
+int hgm_circuit_append_op(hgm_circuit *c, int target, int64_t cmask, int64_t cval, const double m[8]);
+/* Width of the last parsed step (DGM::qubits after genGroups). */
+int hgm_circuit_qubits(const hgm_circuit *c);
+int64_t hgm_circuit_num_ops(const hgm_circuit *c);
+/* Copies the compiled op list out (arrays of num_ops entries; m: 8 per op). */
+int hgm_circuit_get_ops(const hgm_circuit *c, int32_t *target, int64_t *cmask, int64_t *cval, double *m);
+/* Exposes the op list as a NULL-terminated array of reference-layout PTs
+ * (struct hgm_ref_pt of hgm_dropin.h) whose matrices have the given
+ * precision; owned by the circuit, valid until the next change. */
+void *hgm_circuit_ref_pts(hgm_circuit *c, int precision);
+
+/* ---- plans: op list -> state passes ------------------------------------ */
+
+typedef struct hgm_plan_opts {
+    int precision;   /* HGM_F64 / HGM_F32 */
+    int warp_bits;   /* tile = 2^(10+warp_bits) amplitudes; -1 = default */
+    int low_bits;    /* contiguous low index bits kept in every tile; -1 = default */
+    int fuse;        /* 1 = fuse adjacent gates on the same target and controls */
+    int window;      /* scheduling look-ahead in ops; <=0 = default */
+    int renorm_every;/* FP32: rescale to unit norm every k passes (0 = never) */
+} hgm_plan_opts;
+
+void hgm_plan_default_opts(hgm_plan_opts *o, int precision);
+int hgm_plan_create(const hgm_circuit *c, int qubits, const hgm_plan_opts *opts, hgm_plan **out);
+/* Same, from a reference-layout NULL-terminated PT list (hgm_ref_pt**). */
+int hgm_plan_create_from_ref_pts(void *const *pts, int pt_precision, int qubits, const hgm_plan_opts *opts,
+                                 hgm_plan **out);
+void hgm_plan_free(hgm_plan *p);
+/* Plan statistics: ops after fusion, passes, phases, transposes. */
+int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes);
+
+/* ---- device-resident states -------------------------------------------- */
+
+int hgm_state_create(int qubits, int precision, hgm_state **out);
+void hgm_state_free(hgm_state *s);
+int hgm_state_qubits(const hgm_state *s);
+int hgm_state_precision(const hgm_state *s);
+void *hgm_state_device_ptr(hgm_state *s);
+/* |index> (DGM::setMemoryValue, src/core/dgm_core.cpp:63-65). */
+int hgm_state_set_basis(hgm_state *s, int64_t index);
+/* Host <-> device copies of the whole state (bytes = 2^n * amplitude size). */
+int hgm_state_upload(hgm_state *s, const void *host, int64_t bytes);
+int hgm_state_download(const hgm_state *s, void *host, int64_t bytes);
+
+/* ---- execution ---------------------------------------------------------- */
+
+/* Applies the plan `iterations` times on `stream` (0 = the library stream). */
+int hgm_execute(hgm_state *s, const hgm_plan *p, int iterations, void *stream);
+
+/* ---- device-resident measurement (FP64 reductions) ---------------------- */
+
+/* sum |a|^2 */
+int hgm_norm(hgm_state *s, double *out);
+/* Probability that index bit `bit` is 1 (DGM::measure's sums, dgm_core.cpp:79-84). */
+int hgm_prob_one(hgm_state *s, int bit, double *out);
+/* DGM::measure(qubit) (dgm_core.cpp:69-125) on the device: outcome 0 if
+ * P(0) > sample else 1, then collapse and renormalise.  Returns the outcome
+ * and the probability of that outcome. */
+int hgm_measure_qubit(hgm_state *s, int qubit, double sample, int *outcome, double *prob);
+/* Marginal distribution over the index bits in `mask`: argmax of
+ * sum over the other bits of |a|^2 (ties -> lowest index). */
+int hgm_marginal_argmax(hgm_state *s, uint64_t mask, int64_t *arg, double *prob);
+/* <a|b> accumulated in FP64 (a, b may differ in precision, same qubits). */
+int hgm_inner(hgm_state *a, hgm_state *b, double *re, double *im);
+/* max_i |a_i - b_i| */
+int hgm_max_abs_diff(hgm_state *a, hgm_state *b, double *out);
+/* Multiplies every amplitude by `scale`. */
+int hgm_scale(hgm_state *s, double scale);
+
+/* ---- timing (CUDA events on the library stream) ------------------------- */
+
+/* Records an event pair around everything queued between start and stop. */
+int hgm_timer_start(void);
+int hgm_timer_stop(double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HGM_B200_H */

@@ -1,0 +1,108 @@
+// The reference's GPU-backend C-ABI on top of the engine (include/hgm_dropin.h).
+//
+// Compiled twice: without HGM_DROPIN_F64 into libhgm_dropin_f32.so (for the
+// unmodified, FP32 reference) and with it into libhgm_dropin_f64.so (for the
+// FP64-widened reference).  Replaces the reference's src/core/kernel.cu at
+// link time (makefile:51-61).
+//
+// Call semantics kept from src/core/kernel.cu:131-316: the host state is
+// copied in, the PT list is applied `iterations` times, the state is copied
+// back in place and the same pointer is returned; any failure prints a
+// message and exits with status 1 (kernel.cu:439-447).  Unlike the
+// reference, the device buffer is kept between calls of the same size and
+// precision (one cudaMalloc per process instead of one per call).
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+
+#include "hgm_b200.h"
+#include "hgm_dropin.h"
+
+#ifdef HGM_DROPIN_F64
+static const int kPrecision = HGM_F64;
+#else
+static const int kPrecision = HGM_F32;
+#endif
+
+namespace {
+
+std::mutex g_mu;
+hgm_state *g_state = nullptr;
+
+[[noreturn]] void die(const char *what) {
+    printf("hgm_b200: %s: %s\n", what, hgm_last_error());
+    fflush(stdout);
+    exit(1);
+}
+
+}  // namespace
+
+extern "C" {
+
+bool setDevice(int device_id) { return hgm_init(device_id) != HGM_OK; }
+
+hgm_dropin_amp *GpuExecutionWrapper(hgm_dropin_amp *read_memory, hgm_ref_pt **pts, int qubits, int coalesced_bits,
+                                    int gpu_region_bits, int gpu_count, int block_size, int repeat_count,
+                                    int iterations) {
+    static const bool debug = getenv("HYBRID_DEBUG") != nullptr;
+    auto t_start = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lk(g_mu);
+
+    // DGM::validateTuning's GPU rules (src/core/dgm_core.cpp:199-223), kept
+    // at this edge for callers that bypass DGM::execute.
+    if (2L * block_size * repeat_count != (1L << gpu_region_bits)) {
+        printf("Erro de tuning: 2*block_size*repeat_count (%ld) precisa ser igual a 2^gpu_region_bits (%ld)\n",
+               2L * block_size * repeat_count, 1L << gpu_region_bits);
+        exit(1);
+    }
+    if (gpu_region_bits < coalesced_bits) {
+        printf("Erro de tuning: gpu_region_bits (%d) precisa ser >= gpu_coalesced_bits (%d)\n", gpu_region_bits,
+               coalesced_bits);
+        exit(1);
+    }
+    if (gpu_count > 1) {
+        static bool told = false;
+        if (!told) fprintf(stderr, "hgm_b200: gpu_count=%d requested; running on one GPU\n", gpu_count);
+        told = true;
+    }
+    if (read_memory == nullptr) {
+        printf("hgm_b200: device-resident (hybrid) states are not provided\n");
+        exit(1);
+    }
+    if (pts == nullptr) die("null PT list");
+
+    hgm_plan_opts opts;
+    hgm_plan_default_opts(&opts, kPrecision);
+    hgm_plan *plan = nullptr;
+    if (hgm_plan_create_from_ref_pts(reinterpret_cast<void *const *>(pts), kPrecision, qubits, &opts, &plan))
+        die("planning");
+    if (g_state && (hgm_state_qubits(g_state) != qubits)) {
+        hgm_state_free(g_state);
+        g_state = nullptr;
+    }
+    if (!g_state && hgm_state_create(qubits, kPrecision, &g_state)) die("state allocation");
+    const int64_t bytes = (int64_t(1) << qubits) * (int64_t)sizeof(hgm_dropin_amp);
+    if (hgm_state_upload(g_state, read_memory, bytes)) die("copy to device");
+    if (hgm_execute(g_state, plan, iterations, nullptr)) die("execution");
+    if (hgm_state_download(g_state, read_memory, bytes)) die("copy to host");
+    hgm_plan_free(plan);
+
+    if (debug) {
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+        fprintf(stderr, "[GPUEXEC]   qubits=%d elapsed_ms=%.3f\n", qubits, ms);
+    }
+    return read_memory;
+}
+
+bool ProjectState(hgm_dropin_amp *, int, int, long, long, int) {
+    fprintf(stderr, "hgm_b200: the hybrid CPU+GPU mode (ProjectState) is not provided.\n");
+    return false;
+}
+
+bool GetState(hgm_dropin_amp *, int, int, long, long, int) {
+    fprintf(stderr, "hgm_b200: the hybrid CPU+GPU mode (GetState) is not provided.\n");
+    return false;
+}
+
+}  // extern "C"

@@ -1,0 +1,224 @@
+// C-ABI of the engine: runtime, plans, device states, execution and
+// device-resident measurement (include/hgm_b200.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "hgm_dropin_layout.h"
+#include "hgm_internal.h"
+
+using namespace hgm;
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(e == cudaErrorMemoryAllocation ? HGM_ERR_NOMEM : HGM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+template <typename Real>
+void ops_from_ref_pts(void *const *pts, std::vector<Op> &out) {
+    for (long i = 0; pts[i] != nullptr; i++) {
+        const RefPTLayout *pt = reinterpret_cast<const RefPTLayout *>(pts[i]);
+        const Real *m = reinterpret_cast<const Real *>(pt->matrix);
+        Op op;
+        op.target = pt->target_bit;
+        op.cmask = (uint64_t)pt->control_mask;
+        op.cval = (uint64_t)pt->control_value;
+        for (int k = 0; k < 4; k++) op.m[k] = cplx((double)m[2 * k], (double)m[2 * k + 1]);
+        out.push_back(op);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hgm_init(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    e = cudaFree(0);
+    if (e != cudaSuccess) return cuda_fail(e, "context init");
+    return default_stream() ? HGM_OK : HGM_ERR_CUDA;
+}
+
+int hgm_synchronize(void) {
+    cudaError_t e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? HGM_OK : cuda_fail(e, "cudaDeviceSynchronize");
+}
+
+int hgm_mem_info(int64_t *free_bytes, int64_t *total_bytes) {
+    size_t f = 0, t = 0;
+    cudaError_t e = cudaMemGetInfo(&f, &t);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemGetInfo");
+    if (free_bytes) *free_bytes = (int64_t)f;
+    if (total_bytes) *total_bytes = (int64_t)t;
+    return HGM_OK;
+}
+
+void hgm_plan_default_opts(hgm_plan_opts *o, int precision) {
+    o->precision = precision;
+    o->warp_bits = -1;
+    o->low_bits = -1;
+    o->fuse = 1;
+    o->window = 0;
+    o->renorm_every = precision == HGM_F32 ? 64 : 0;
+}
+
+static int finish_plan(const std::vector<Op> &ops, int qubits, const hgm_plan_opts *opts, hgm_plan **out) {
+    if (!out) return fail(HGM_ERR_INVALID, "null output");
+    hgm_plan_opts o;
+    if (opts) o = *opts;
+    else hgm_plan_default_opts(&o, HGM_F64);
+    if (o.precision != HGM_F64 && o.precision != HGM_F32) return fail(HGM_ERR_INVALID, "bad precision");
+    std::unique_ptr<Plan> p(new Plan());
+    int rc = build_plan(ops, qubits, o, p.get());
+    if (rc) return rc;
+    *out = reinterpret_cast<hgm_plan *>(p.release());
+    return HGM_OK;
+}
+
+int hgm_plan_create(const hgm_circuit *c, int qubits, const hgm_plan_opts *opts, hgm_plan **out) {
+    if (!c) return fail(HGM_ERR_INVALID, "null circuit");
+    return finish_plan(reinterpret_cast<const Circuit *>(c)->ops, qubits, opts, out);
+}
+
+int hgm_plan_create_from_ref_pts(void *const *pts, int pt_precision, int qubits, const hgm_plan_opts *opts,
+                                 hgm_plan **out) {
+    if (!pts) return fail(HGM_ERR_INVALID, "null PT list");
+    std::vector<Op> ops;
+    if (pt_precision == HGM_F64) ops_from_ref_pts<double>(pts, ops);
+    else ops_from_ref_pts<float>(pts, ops);
+    return finish_plan(ops, qubits, opts, out);
+}
+
+void hgm_plan_free(hgm_plan *p) { delete reinterpret_cast<Plan *>(p); }
+
+int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes) {
+    if (!p) return fail(HGM_ERR_INVALID, "null plan");
+    const Plan *pl = reinterpret_cast<const Plan *>(p);
+    if (n_ops) *n_ops = pl->n_ops;
+    if (n_passes) *n_passes = pl->small ? (pl->n_small_ops ? 1 : 0) : (int64_t)pl->passes.size();
+    if (n_phases) *n_phases = (int64_t)pl->phases.size();
+    if (n_transposes) *n_transposes = pl->n_transposes;
+    return HGM_OK;
+}
+
+int hgm_state_create(int qubits, int precision, hgm_state **out) {
+    if (!out) return fail(HGM_ERR_INVALID, "null output");
+    if (qubits < 1 || qubits > 34) return fail(HGM_ERR_UNSUPPORTED, "qubits=%d outside 1..34", qubits);
+    if (precision != HGM_F64 && precision != HGM_F32) return fail(HGM_ERR_INVALID, "bad precision");
+    if (!default_stream()) return HGM_ERR_CUDA;
+    std::unique_ptr<State> s(new State());
+    s->qubits = qubits;
+    s->precision = precision;
+    cudaError_t e = cudaMalloc(&s->d, (size_t)s->bytes());
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "state allocation");
+    }
+    *out = reinterpret_cast<hgm_state *>(s.release());
+    return HGM_OK;
+}
+
+void hgm_state_free(hgm_state *s) {
+    State *st = reinterpret_cast<State *>(s);
+    if (!st) return;
+    if (st->d) cudaFree(st->d);
+    delete st;
+}
+
+int hgm_state_qubits(const hgm_state *s) { return s ? reinterpret_cast<const State *>(s)->qubits : 0; }
+int hgm_state_precision(const hgm_state *s) { return s ? reinterpret_cast<const State *>(s)->precision : -1; }
+void *hgm_state_device_ptr(hgm_state *s) { return s ? reinterpret_cast<State *>(s)->d : nullptr; }
+
+int hgm_state_set_basis(hgm_state *s, int64_t index) {
+    if (!s) return fail(HGM_ERR_INVALID, "null state");
+    return launch_set_basis(reinterpret_cast<State *>(s), index, nullptr);
+}
+
+int hgm_state_upload(hgm_state *s, const void *host, int64_t bytes) {
+    State *st = reinterpret_cast<State *>(s);
+    if (!st || !host) return fail(HGM_ERR_INVALID, "null argument");
+    if (bytes != st->bytes()) return fail(HGM_ERR_INVALID, "upload of %lld bytes into a %lld-byte state",
+                                          (long long)bytes, (long long)st->bytes());
+    cudaStream_t stream = (cudaStream_t)default_stream();
+    cudaError_t e = cudaMemcpyAsync(st->d, host, (size_t)bytes, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    return e == cudaSuccess ? HGM_OK : cuda_fail(e, "state upload");
+}
+
+int hgm_state_download(const hgm_state *s, void *host, int64_t bytes) {
+    const State *st = reinterpret_cast<const State *>(s);
+    if (!st || !host) return fail(HGM_ERR_INVALID, "null argument");
+    if (bytes != st->bytes()) return fail(HGM_ERR_INVALID, "download of %lld bytes from a %lld-byte state",
+                                          (long long)bytes, (long long)st->bytes());
+    cudaStream_t stream = (cudaStream_t)default_stream();
+    cudaError_t e = cudaMemcpyAsync(host, st->d, (size_t)bytes, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    return e == cudaSuccess ? HGM_OK : cuda_fail(e, "state download");
+}
+
+int hgm_execute(hgm_state *s, const hgm_plan *p, int iterations, void *stream) {
+    if (!s || !p) return fail(HGM_ERR_INVALID, "null argument");
+    if (iterations < 0) return fail(HGM_ERR_INVALID, "negative iterations");
+    Plan *pl = const_cast<Plan *>(reinterpret_cast<const Plan *>(p));
+    int rc = upload_plan(pl);
+    if (rc) return rc;
+    if (iterations == 0) return HGM_OK;
+    return launch_plan(reinterpret_cast<State *>(s), pl, iterations, stream);
+}
+
+int hgm_norm(hgm_state *s, double *out) {
+    if (!s) return fail(HGM_ERR_INVALID, "null state");
+    return reduce_norm(reinterpret_cast<State *>(s), out, nullptr);
+}
+
+int hgm_prob_one(hgm_state *s, int bit, double *out) {
+    if (!s) return fail(HGM_ERR_INVALID, "null state");
+    return reduce_prob_one(reinterpret_cast<State *>(s), bit, out, nullptr);
+}
+
+int hgm_measure_qubit(hgm_state *s, int qubit, double sample, int *outcome, double *prob) {
+    State *st = reinterpret_cast<State *>(s);
+    if (!st) return fail(HGM_ERR_INVALID, "null state");
+    if (qubit < 0 || qubit >= st->qubits) return fail(HGM_ERR_INVALID, "qubit %d outside state", qubit);
+    const int bit = st->qubits - 1 - qubit;
+    double total = 0, one = 0;
+    int rc = reduce_norm(st, &total, nullptr);
+    if (!rc) rc = reduce_prob_one(st, bit, &one, nullptr);
+    if (rc) return rc;
+    const double zero = total - one;
+    // DGM::measure: outcome 0 iff P(0) > sample (dgm_core.cpp:97-113)
+    const int value = (zero > sample) ? 0 : 1;
+    const double p = value ? one : zero;
+    if (!(p > 0)) return fail(HGM_ERR_INVALID, "measured outcome has zero probability");
+    rc = collapse(st, bit, value, 1.0 / std::sqrt(p), nullptr);
+    if (rc) return rc;
+    if (outcome) *outcome = value;
+    if (prob) *prob = p;
+    return HGM_OK;
+}
+
+int hgm_marginal_argmax(hgm_state *s, uint64_t mask, int64_t *arg, double *prob) {
+    if (!s) return fail(HGM_ERR_INVALID, "null state");
+    return marginal_argmax(reinterpret_cast<State *>(s), mask, arg, prob, nullptr);
+}
+
+int hgm_inner(hgm_state *a, hgm_state *b, double *re, double *im) {
+    if (!a || !b) return fail(HGM_ERR_INVALID, "null state");
+    return inner(reinterpret_cast<State *>(a), reinterpret_cast<State *>(b), re, im, nullptr);
+}
+
+int hgm_max_abs_diff(hgm_state *a, hgm_state *b, double *out) {
+    if (!a || !b) return fail(HGM_ERR_INVALID, "null state");
+    return max_abs_diff(reinterpret_cast<State *>(a), reinterpret_cast<State *>(b), out, nullptr);
+}
+
+int hgm_scale(hgm_state *s, double f) {
+    if (!s) return fail(HGM_ERR_INVALID, "null state");
+    return scale_state(reinterpret_cast<State *>(s), f, nullptr);
+}
+
+}  // extern "C"

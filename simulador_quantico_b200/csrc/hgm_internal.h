@@ -1,0 +1,157 @@
+// Internal declarations shared by the engine's host (C++) and device (CUDA)
+// translation units.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "hgm_b200.h"
+
+namespace hgm {
+
+using cplx = std::complex<double>;
+
+// Matrix classes, the reference's PT::matrixType (src/core/common.cpp:33-38)
+// by exact zero tests.
+enum MatClass : int { MC_DENSE = 0, MC_DIAG = 1, MC_ANTI = 2 };
+
+// One compiled controlled 1-qubit gate (the fields of struct PT the engines
+// read, include/core/common.h:57-90).  Matrices are kept in FP64.
+struct Op {
+    int target = 0;
+    uint64_t cmask = 0, cval = 0;
+    cplx m[4];
+};
+
+MatClass classify(const cplx m[4]);
+
+// ---- errors ---------------------------------------------------------------
+void set_error(const char *fmt, ...);
+int fail(int code, const char *fmt, ...);
+
+// ---- circuit language ------------------------------------------------------
+struct Circuit {
+    std::map<std::string, std::vector<cplx>> gates;
+    std::vector<Op> ops;
+    int qubits = 0;
+    // reference-layout PT export (hgm_circuit_ref_pts)
+    std::vector<unsigned char> pt_storage;
+    std::vector<void *> pt_ptrs;
+    std::vector<unsigned char> mat_storage;
+
+    Circuit();
+    bool add_gate(const std::string &name, const cplx m[4]);
+    int set_function(const std::string &steps, int iterations, bool reset);
+};
+
+// ---- kernel-side encodings (shared with kernels.cuh) ----------------------
+
+// Register-phase layouts of a warp tile (see kernels.cuh).
+enum Layout : int32_t { LAYOUT_C = 0, LAYOUT_B = 1, LAYOUT_A = 2 };
+
+enum DevKind : int32_t {
+    K_DENSE = 0,   // general 2x2
+    K_REAL = 1,    // all four entries real
+    K_DIAG = 2,    // diag(m00, m11)
+    K_PHASE = 3,   // diag(1, m11)
+    K_ANTI = 4,    // [[0, m01], [m10, 0]]
+    K_SWAP = 5,    // [[0, 1], [1, 0]]
+};
+
+// Target location codes inside a phase: 0..4 register bit, 8+q thread bit q
+// (lane bits 0..4, warp bits 5..), 64+g a non-tile index bit g.
+constexpr int TPOS_THREAD = 8;
+constexpr int TPOS_GLOBAL = 64;
+
+template <typename Real>
+struct alignas(16) DevOp {
+    int32_t kind, tpos;
+    uint32_t cm_reg, cv_reg;   // controls on register bits
+    uint32_t cm_thr, cv_thr;   // controls on thread bits (lane | warp << 5)
+    uint64_t cm_glob, cv_glob; // controls on non-tile index bits
+    Real m[8];
+};
+
+struct DevPhase {
+    int32_t layout;
+    int32_t op_begin, op_end;
+    int32_t xwarp;   // 1 if entering this phase needs a cross-warp transpose
+};
+
+constexpr int MAX_TILE_BITS = 16;
+
+struct PassArgs {
+    int32_t n;            // qubits
+    int32_t k;            // tile bits = 10 + W
+    int32_t phase_begin, phase_end;
+    int32_t load_layout, store_layout;
+    int32_t flags;        // PASS_* below
+    int32_t pad;
+    int8_t tb[MAX_TILE_BITS];  // local tile bit -> global index bit
+    uint64_t tile_mask;
+    const DevPhase *phases;
+    const void *ops;      // DevOp<Real>*
+    double *norm_out;     // PASS_NORM: accumulate sum |a|^2 of stored amplitudes
+    const double *scale_in; // PASS_SCALE: multiply loaded amplitudes by 1/sqrt(*scale_in)
+};
+
+constexpr int32_t PASS_NORM = 1;
+constexpr int32_t PASS_SCALE = 2;
+
+// Small-state path (n < 10): whole state in one CTA's shared memory, ops
+// applied one at a time.
+template <typename Real>
+struct SmallOp {
+    int32_t target, kind;
+    uint32_t cmask, cval;
+    Real m[8];
+};
+
+// ---- plan ------------------------------------------------------------------
+struct Plan {
+    int precision = HGM_F64;
+    int qubits = 0;
+    int warp_bits = 0;
+    bool small = false;               // n < 10: single-CTA shared-memory path
+    std::vector<PassArgs> passes;     // device pointers patched after upload
+    std::vector<DevPhase> phases;
+    std::vector<unsigned char> ops_bytes;   // DevOp<Real>[] or SmallOp<Real>[]
+    int64_t n_small_ops = 0;
+    int64_t n_ops = 0, n_transposes = 0;
+    // device copies
+    void *d_phases = nullptr;
+    void *d_ops = nullptr;
+    int renorm_every = 0;
+    double *d_norm = nullptr;         // renormalisation scratch (FP32 plans)
+    ~Plan();
+};
+
+int build_plan(const std::vector<Op> &ops, int qubits, const hgm_plan_opts &opts, Plan *plan);
+int upload_plan(Plan *plan);
+
+// ---- device state ------------------------------------------------------------
+struct State {
+    int qubits = 0;
+    int precision = HGM_F64;
+    void *d = nullptr;
+    int64_t bytes() const { return (int64_t(1) << qubits) * (precision == HGM_F64 ? 16 : 8); }
+};
+
+// ---- launchers (kernels.cu) ----------------------------------------------------
+int launch_plan(State *s, const Plan *p, int iterations, void *stream);
+int launch_set_basis(State *s, int64_t index, void *stream);
+int reduce_norm(State *s, double *out, void *stream);
+int reduce_prob_one(State *s, int bit, double *out, void *stream);
+int collapse(State *s, int bit, int value, double inv_norm, void *stream);
+int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *stream);
+int inner(State *a, State *b, double *re, double *im, void *stream);
+int max_abs_diff(State *a, State *b, double *out, void *stream);
+int scale_state(State *s, double scale, void *stream);
+
+void *default_stream();
+void count_launch(int n = 1);
+
+}  // namespace hgm

@@ -1,0 +1,567 @@
+// Kernels and launchers of the state-vector engine (sm_100a).
+//
+//   pass_kernel<Real, W>   one state pass of a plan (kernels.cuh: run_tile)
+//   small_kernel<Real>     states of < 10 qubits: whole state in one CTA's
+//                          shared memory, gates applied one by one
+//   reduce_*               FP64 reductions (norm, bit probability, inner
+//                          product, max |difference|) with a fixed grid and a
+//                          fixed combine order, so a result does not depend
+//                          on what else runs on the device
+//   collapse / scale / set_basis / marginal argmax
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <mutex>
+
+#include "kernels.cuh"
+
+namespace hgm {
+
+// ---------------------------------------------------------------------------
+// context: one library stream, a small scratch area for reductions
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr int RED_BLOCKS = 1184;   // 8 x 148 SMs
+constexpr int RED_THREADS = 256;
+
+struct Ctx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    double *partials = nullptr;    // RED_BLOCKS * 2 doubles
+    long long *partial_idx = nullptr;
+    double *result = nullptr;      // 4 doubles (device)
+    double *host_result = nullptr; // 4 doubles (pinned)
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+};
+Ctx g_ctx;
+std::mutex g_ctx_mu;
+std::atomic<long long> g_launches{0};
+}  // namespace
+
+void count_launch(int n) { g_launches += n; }
+
+static int ensure_ctx() {
+    if (g_ctx.stream) return HGM_OK;
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (g_ctx.stream) return HGM_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    g_ctx.device = dev;
+    cudaStream_t s;
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(HGM_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    if ((e = cudaMalloc(&g_ctx.partials, RED_BLOCKS * 2 * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&g_ctx.partial_idx, RED_BLOCKS * sizeof(long long))) != cudaSuccess ||
+        (e = cudaMalloc(&g_ctx.result, 4 * sizeof(double))) != cudaSuccess ||
+        (e = cudaMallocHost(&g_ctx.host_result, 4 * sizeof(double))) != cudaSuccess ||
+        (e = cudaEventCreate(&g_ctx.t0)) != cudaSuccess || (e = cudaEventCreate(&g_ctx.t1)) != cudaSuccess)
+        return fail(HGM_ERR_CUDA, "context setup: %s", cudaGetErrorString(e));
+    g_ctx.stream = s;
+    return HGM_OK;
+}
+
+void *default_stream() {
+    if (ensure_ctx() != HGM_OK) return nullptr;
+    return g_ctx.stream;
+}
+
+static inline cudaStream_t pick(void *stream) {
+    return stream ? (cudaStream_t)stream : (cudaStream_t)default_stream();
+}
+
+static inline int check(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return HGM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pass kernels
+// ---------------------------------------------------------------------------
+
+template <typename Real, int W>
+__global__ void __launch_bounds__(32 << W) pass_kernel(typename V2<Real>::T *__restrict__ state, const PassArgs pa) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    run_tile<Real, W>(state, pa, blockIdx.x, reinterpret_cast<typename V2<Real>::T *>(smem_raw));
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(256) small_kernel(typename V2<Real>::T *__restrict__ state, int n,
+                                                    const SmallOp<Real> *__restrict__ ops, long long n_ops,
+                                                    int iterations) {
+    using A2 = typename V2<Real>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    A2 *sm = reinterpret_cast<A2 *>(smem_raw);
+    const int N = 1 << n, half = N >> 1;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) sm[i] = state[i];
+    __syncthreads();
+    for (int it = 0; it < iterations; it++) {
+        for (long long k = 0; k < n_ops; k++) {
+            const SmallOp<Real> &o = ops[k];
+            const int t = o.target;
+            const uint32_t cm = o.cmask, cv = o.cval;
+            const Real m0r = o.m[0], m0i = o.m[1], m1r = o.m[2], m1i = o.m[3];
+            const Real m2r = o.m[4], m2i = o.m[5], m3r = o.m[6], m3i = o.m[7];
+            for (int p = threadIdx.x; p < half; p += blockDim.x) {
+                const int i0 = ((p >> t) << (t + 1)) | (p & ((1 << t) - 1));
+                const int i1 = i0 | (1 << t);
+                if (((uint32_t)i0 & cm) != cv) continue;
+                const A2 x = sm[i0], y = sm[i1];
+                A2 o0, o1;
+                o0.x = m0r * x.x - m0i * x.y + m1r * y.x - m1i * y.y;
+                o0.y = m0r * x.y + m0i * x.x + m1r * y.y + m1i * y.x;
+                o1.x = m2r * x.x - m2i * x.y + m3r * y.x - m3i * y.y;
+                o1.y = m2r * x.y + m2i * x.x + m3r * y.y + m3i * y.x;
+                sm[i0] = o0;
+                sm[i1] = o1;
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < N; i += blockDim.x) state[i] = sm[i];
+}
+
+template <typename Real, int W>
+static int setup_pass_kernel() {
+    static bool done = false;
+    if (done) return HGM_OK;
+    const int smem = (1 << (10 + W)) * (int)sizeof(typename V2<Real>::T);
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<Real, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    done = true;
+    return HGM_OK;
+}
+
+template <typename Real, int W>
+static int launch_pass(void *state, const PassArgs &pa, cudaStream_t st) {
+    int rc = setup_pass_kernel<Real, W>();
+    if (rc) return rc;
+    const uint64_t tiles = 1ull << (pa.n - pa.k);
+    const int smem = (1 << (10 + W)) * (int)sizeof(typename V2<Real>::T);
+    pass_kernel<Real, W><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<typename V2<Real>::T *>(state), pa);
+    count_launch();
+    return HGM_OK;
+}
+
+template <typename Real>
+static int launch_pass_w(int W, void *state, const PassArgs &pa, cudaStream_t st) {
+    switch (W) {
+        case 0: return launch_pass<Real, 0>(state, pa, st);
+        case 1: return launch_pass<Real, 1>(state, pa, st);
+        case 2: return launch_pass<Real, 2>(state, pa, st);
+        default: return launch_pass<Real, 3>(state, pa, st);
+    }
+}
+
+template <typename Real>
+static int launch_small(State *s, const Plan *p, int iterations, cudaStream_t st) {
+    const int smem = (1 << s->qubits) * (int)sizeof(typename V2<Real>::T);
+    small_kernel<Real><<<1, 256, smem, st>>>(reinterpret_cast<typename V2<Real>::T *>(s->d), s->qubits,
+                                             reinterpret_cast<const SmallOp<Real> *>(p->d_ops), p->n_small_ops,
+                                             iterations);
+    count_launch();
+    return check("small_kernel launch");
+}
+
+int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
+    if (s->qubits != p->qubits) return fail(HGM_ERR_INVALID, "plan is for %d qubits, state has %d", p->qubits, s->qubits);
+    if (s->precision != p->precision) return fail(HGM_ERR_INVALID, "plan and state precision differ");
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    if (p->small) return p->n_small_ops ? (p->precision == HGM_F64 ? launch_small<double>(s, p, iterations, st)
+                                                                 : launch_small<float>(s, p, iterations, st))
+                                       : HGM_OK;
+    const size_t np = p->passes.size();
+    const int R = p->renorm_every;
+    int64_t global_pass = 0;
+    const int64_t total = (int64_t)np * iterations;
+    int slot = 0;
+    bool scale_next = false;
+    int scale_slot = 0;
+    for (int it = 0; it < iterations; it++) {
+        for (size_t i = 0; i < np; i++, global_pass++) {
+            PassArgs pa = p->passes[i];
+            pa.flags = 0;
+            if (scale_next) {
+                pa.flags |= PASS_SCALE;
+                pa.scale_in = p->d_norm + scale_slot;
+                scale_next = false;
+            }
+            if (R > 0 && ((global_pass + 1) % R == 0) && global_pass + 1 < total) {
+                pa.flags |= PASS_NORM;
+                pa.norm_out = p->d_norm + slot;
+                cudaMemsetAsync(pa.norm_out, 0, sizeof(double), st);
+                scale_next = true;
+                scale_slot = slot;
+                slot = (slot + 1) % 64;
+            }
+            int rc = p->precision == HGM_F64 ? launch_pass_w<double>(p->warp_bits, s->d, pa, st)
+                                             : launch_pass_w<float>(p->warp_bits, s->d, pa, st);
+            if (rc) return rc;
+        }
+    }
+    return check("pass_kernel launch");
+}
+
+// ---------------------------------------------------------------------------
+// plan upload
+// ---------------------------------------------------------------------------
+
+Plan::~Plan() {
+    if (d_phases) cudaFree(d_phases);
+    if (d_ops) cudaFree(d_ops);
+    if (d_norm) cudaFree(d_norm);
+}
+
+int upload_plan(Plan *p) {
+    if (p->d_ops || (p->ops_bytes.empty() && p->phases.empty() && !p->renorm_every)) return HGM_OK;
+    if (ensure_ctx()) return HGM_ERR_CUDA;
+    cudaError_t e;
+    if (!p->ops_bytes.empty()) {
+        if ((e = cudaMalloc(&p->d_ops, p->ops_bytes.size())) != cudaSuccess)
+            return fail(HGM_ERR_NOMEM, "plan ops: %s", cudaGetErrorString(e));
+        if ((e = cudaMemcpy(p->d_ops, p->ops_bytes.data(), p->ops_bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(HGM_ERR_CUDA, "plan ops copy: %s", cudaGetErrorString(e));
+    }
+    if (!p->phases.empty()) {
+        size_t b = p->phases.size() * sizeof(DevPhase);
+        if ((e = cudaMalloc(&p->d_phases, b)) != cudaSuccess) return fail(HGM_ERR_NOMEM, "plan phases: %s", cudaGetErrorString(e));
+        if ((e = cudaMemcpy(p->d_phases, p->phases.data(), b, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(HGM_ERR_CUDA, "plan phases copy: %s", cudaGetErrorString(e));
+    }
+    if (p->renorm_every > 0) {
+        if ((e = cudaMalloc(&p->d_norm, 64 * sizeof(double))) != cudaSuccess)
+            return fail(HGM_ERR_NOMEM, "plan norm slots: %s", cudaGetErrorString(e));
+    }
+    for (PassArgs &pa : p->passes) {
+        pa.phases = reinterpret_cast<const DevPhase *>(p->d_phases);
+        pa.ops = p->d_ops;
+    }
+    return HGM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// elementwise kernels
+// ---------------------------------------------------------------------------
+
+template <typename Real>
+__global__ void set_basis_kernel(typename V2<Real>::T *s, long long N, long long index) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        typename V2<Real>::T v;
+        v.x = (i == index) ? (Real)1 : (Real)0;
+        v.y = 0;
+        s[i] = v;
+    }
+}
+
+template <typename Real>
+__global__ void collapse_kernel(typename V2<Real>::T *s, long long N, int bit, int value, double inv_norm) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        typename V2<Real>::T v = s[i];
+        if ((int)((i >> bit) & 1) == value) {
+            v.x = (Real)(v.x * inv_norm);
+            v.y = (Real)(v.y * inv_norm);
+        } else {
+            v.x = 0;
+            v.y = 0;
+        }
+        s[i] = v;
+    }
+}
+
+template <typename Real>
+__global__ void scale_kernel(typename V2<Real>::T *s, long long N, double f) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        typename V2<Real>::T v = s[i];
+        v.x = (Real)(v.x * f);
+        v.y = (Real)(v.y * f);
+        s[i] = v;
+    }
+}
+
+static unsigned grid_for(long long N) {
+    long long g = (N + 255) / 256;
+    return (unsigned)(g < RED_BLOCKS ? (g < 1 ? 1 : g) : RED_BLOCKS);
+}
+
+int launch_set_basis(State *s, int64_t index, void *stream) {
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    long long N = 1ll << s->qubits;
+    if (index < 0 || index >= N) return fail(HGM_ERR_INVALID, "basis index %lld outside state", (long long)index);
+    if (s->precision == HGM_F64) set_basis_kernel<double><<<grid_for(N), 256, 0, st>>>((double2 *)s->d, N, index);
+    else set_basis_kernel<float><<<grid_for(N), 256, 0, st>>>((float2 *)s->d, N, index);
+    count_launch();
+    return check("set_basis");
+}
+
+int collapse(State *s, int bit, int value, double inv_norm, void *stream) {
+    cudaStream_t st = pick(stream);
+    long long N = 1ll << s->qubits;
+    if (s->precision == HGM_F64) collapse_kernel<double><<<grid_for(N), 256, 0, st>>>((double2 *)s->d, N, bit, value, inv_norm);
+    else collapse_kernel<float><<<grid_for(N), 256, 0, st>>>((float2 *)s->d, N, bit, value, inv_norm);
+    count_launch();
+    return check("collapse");
+}
+
+int scale_state(State *s, double f, void *stream) {
+    cudaStream_t st = pick(stream);
+    long long N = 1ll << s->qubits;
+    if (s->precision == HGM_F64) scale_kernel<double><<<grid_for(N), 256, 0, st>>>((double2 *)s->d, N, f);
+    else scale_kernel<float><<<grid_for(N), 256, 0, st>>>((float2 *)s->d, N, f);
+    count_launch();
+    return check("scale");
+}
+
+// ---------------------------------------------------------------------------
+// FP64 reductions (fixed grid, fixed combine order)
+// ---------------------------------------------------------------------------
+
+enum RedMode { RED_NORM = 0, RED_PROB1 = 1, RED_INNER = 2, RED_MAXDIFF = 3 };
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <typename RA, typename RB, int MODE>
+__global__ void __launch_bounds__(RED_THREADS) reduce_kernel(const typename V2<RA>::T *__restrict__ a,
+                                                              const typename V2<RB>::T *__restrict__ b, long long N,
+                                                              int bit, double *partials) {
+    double s0 = 0.0, s1 = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const typename V2<RA>::T x = a[i];
+        if (MODE == RED_NORM) {
+            s0 += (double)x.x * x.x + (double)x.y * x.y;
+        } else if (MODE == RED_PROB1) {
+            if ((i >> bit) & 1) s0 += (double)x.x * x.x + (double)x.y * x.y;
+        } else if (MODE == RED_INNER) {
+            const typename V2<RB>::T y = b[i];
+            // conj(x) * y
+            s0 += (double)x.x * y.x + (double)x.y * y.y;
+            s1 += (double)x.x * y.y - (double)x.y * y.x;
+        } else {
+            const typename V2<RB>::T y = b[i];
+            const double dr = (double)x.x - (double)y.x, di = (double)x.y - (double)y.y;
+            s0 = fmax(s0, sqrt(dr * dr + di * di));
+        }
+    }
+    __shared__ double sh[2][RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (MODE == RED_MAXDIFF) s0 = warp_max(s0);
+    else {
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+    }
+    if (lane == 0) {
+        sh[0][w] = s0;
+        sh[1][w] = s1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int k = 0; k < RED_THREADS / 32; k++) {
+            if (MODE == RED_MAXDIFF) t0 = fmax(t0, sh[0][k]);
+            else t0 += sh[0][k];
+            t1 += sh[1][k];
+        }
+        partials[2 * blockIdx.x] = t0;
+        partials[2 * blockIdx.x + 1] = t1;
+    }
+}
+
+template <int MODE>
+__global__ void reduce_final(const double *partials, int nblocks, double *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int k = 0; k < nblocks; k++) {
+            if (MODE == RED_MAXDIFF) t0 = fmax(t0, partials[2 * k]);
+            else t0 += partials[2 * k];
+            t1 += partials[2 * k + 1];
+        }
+        out[0] = t0;
+        out[1] = t1;
+    }
+}
+
+template <typename RA, typename RB, int MODE>
+static int run_reduce(const void *a, const void *b, int qubits, int bit, double *o0, double *o1, cudaStream_t st) {
+    const long long N = 1ll << qubits;
+    const unsigned g = grid_for(N);
+    reduce_kernel<RA, RB, MODE><<<g, RED_THREADS, 0, st>>>((const typename V2<RA>::T *)a,
+                                                           (const typename V2<RB>::T *)b, N, bit, g_ctx.partials);
+    reduce_final<MODE><<<1, 32, 0, st>>>(g_ctx.partials, (int)g, g_ctx.result);
+    count_launch(2);
+    cudaMemcpyAsync(g_ctx.host_result, g_ctx.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "reduction: %s", cudaGetErrorString(e));
+    if (o0) *o0 = g_ctx.host_result[0];
+    if (o1) *o1 = g_ctx.host_result[1];
+    return HGM_OK;
+}
+
+int reduce_norm(State *s, double *out, void *stream) {
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    return s->precision == HGM_F64 ? run_reduce<double, double, RED_NORM>(s->d, nullptr, s->qubits, 0, out, nullptr, st)
+                                   : run_reduce<float, float, RED_NORM>(s->d, nullptr, s->qubits, 0, out, nullptr, st);
+}
+
+int reduce_prob_one(State *s, int bit, double *out, void *stream) {
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    if (bit < 0 || bit >= s->qubits) return fail(HGM_ERR_INVALID, "bit %d outside state", bit);
+    return s->precision == HGM_F64 ? run_reduce<double, double, RED_PROB1>(s->d, nullptr, s->qubits, bit, out, nullptr, st)
+                                   : run_reduce<float, float, RED_PROB1>(s->d, nullptr, s->qubits, bit, out, nullptr, st);
+}
+
+template <int MODE>
+static int two_state(State *a, State *b, double *o0, double *o1, cudaStream_t st) {
+    if (a->qubits != b->qubits) return fail(HGM_ERR_INVALID, "states differ in size");
+    if (a->precision == HGM_F64 && b->precision == HGM_F64)
+        return run_reduce<double, double, MODE>(a->d, b->d, a->qubits, 0, o0, o1, st);
+    if (a->precision == HGM_F64) return run_reduce<double, float, MODE>(a->d, b->d, a->qubits, 0, o0, o1, st);
+    if (b->precision == HGM_F64) return run_reduce<float, double, MODE>(a->d, b->d, a->qubits, 0, o0, o1, st);
+    return run_reduce<float, float, MODE>(a->d, b->d, a->qubits, 0, o0, o1, st);
+}
+
+int inner(State *a, State *b, double *re, double *im, void *stream) {
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    return two_state<RED_INNER>(a, b, re, im, st);
+}
+
+int max_abs_diff(State *a, State *b, double *out, void *stream) {
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    return two_state<RED_MAXDIFF>(a, b, out, nullptr, st);
+}
+
+// Marginal argmax: for every value x of the bits in `mask`, p(x) = sum over
+// the other bits of |a|^2; returns the x with the largest p (lowest on ties).
+// Each thread owns marginal values x and walks the complement bits.
+template <typename Real>
+__global__ void __launch_bounds__(RED_THREADS) marginal_kernel(const typename V2<Real>::T *__restrict__ s, int n,
+                                                                unsigned long long mask, int m, double *pbest,
+                                                                long long *ibest) {
+    const unsigned long long comp = ~mask & ((n >= 64) ? ~0ull : ((1ull << n) - 1));
+    const long long M = 1ll << m, C = 1ll << (n - m);
+    double best = -1.0;
+    long long besti = 0;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < M; x += (long long)gridDim.x * blockDim.x) {
+        // deposit x into mask bits
+        unsigned long long base = 0, src = (unsigned long long)x, mm = mask;
+        while (mm) {
+            int g = __ffsll((long long)mm) - 1;
+            mm &= mm - 1;
+            base |= (src & 1ull) << g;
+            src >>= 1;
+        }
+        double p = 0.0;
+        for (long long c = 0; c < C; c++) {
+            unsigned long long idx = base, cs = (unsigned long long)c, cm = comp;
+            while (cm) {
+                int g = __ffsll((long long)cm) - 1;
+                cm &= cm - 1;
+                idx |= (cs & 1ull) << g;
+                cs >>= 1;
+            }
+            const typename V2<Real>::T v = s[idx];
+            p += (double)v.x * v.x + (double)v.y * v.y;
+        }
+        if (p > best) {
+            best = p;
+            besti = x;
+        }
+    }
+    __shared__ double sp[RED_THREADS];
+    __shared__ long long si[RED_THREADS];
+    sp[threadIdx.x] = best;
+    si[threadIdx.x] = besti;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = -1.0;
+        long long bi = 0;
+        for (int k = 0; k < RED_THREADS; k++)
+            if (sp[k] > b || (sp[k] == b && si[k] < bi)) {
+                b = sp[k];
+                bi = si[k];
+            }
+        pbest[blockIdx.x] = b;
+        ibest[blockIdx.x] = bi;
+    }
+}
+
+__global__ void marginal_final(const double *pbest, const long long *ibest, int nb, double *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double b = -1.0;
+        long long bi = 0;
+        for (int k = 0; k < nb; k++)
+            if (pbest[k] > b || (pbest[k] == b && ibest[k] < bi)) {
+                b = pbest[k];
+                bi = ibest[k];
+            }
+        out[0] = b;
+        out[1] = (double)bi;
+    }
+}
+
+int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *stream) {
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    const int n = s->qubits;
+    if (n < 64 && (mask >> n)) return fail(HGM_ERR_INVALID, "mask beyond state bits");
+    const int m = __builtin_popcountll(mask);
+    const long long M = 1ll << m;
+    unsigned g = (unsigned)((M + RED_THREADS - 1) / RED_THREADS);
+    if (g > RED_BLOCKS) g = RED_BLOCKS;
+    if (g < 1) g = 1;
+    if (s->precision == HGM_F64)
+        marginal_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, m, g_ctx.partials, g_ctx.partial_idx);
+    else
+        marginal_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, m, g_ctx.partials, g_ctx.partial_idx);
+    marginal_final<<<1, 32, 0, st>>>(g_ctx.partials, g_ctx.partial_idx, (int)g, g_ctx.result);
+    count_launch(2);
+    cudaMemcpyAsync(g_ctx.host_result, g_ctx.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "marginal argmax: %s", cudaGetErrorString(e));
+    if (prob) *prob = g_ctx.host_result[0];
+    if (arg) *arg = (int64_t)g_ctx.host_result[1];
+    return HGM_OK;
+}
+
+}  // namespace hgm
+
+using namespace hgm;
+
+extern "C" {
+
+int64_t hgm_kernel_launches(void) { return g_launches.load(); }
+
+int hgm_timer_start(void) {
+    if (ensure_ctx()) return HGM_ERR_CUDA;
+    cudaError_t e = cudaEventRecord(g_ctx.t0, g_ctx.stream);
+    return e == cudaSuccess ? HGM_OK : fail(HGM_ERR_CUDA, "event record: %s", cudaGetErrorString(e));
+}
+
+int hgm_timer_stop(double *ms) {
+    if (ensure_ctx()) return HGM_ERR_CUDA;
+    cudaEventRecord(g_ctx.t1, g_ctx.stream);
+    cudaError_t e = cudaEventSynchronize(g_ctx.t1);
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "event sync: %s", cudaGetErrorString(e));
+    float f = 0;
+    cudaEventElapsedTime(&f, g_ctx.t0, g_ctx.t1);
+    if (ms) *ms = f;
+    return HGM_OK;
+}
+
+}  // extern "C"

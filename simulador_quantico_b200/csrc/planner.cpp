@@ -1,0 +1,393 @@
+// Planner: compiled op list -> state passes -> register phases.
+//
+// The reference groups consecutive PTs whose targets fit one
+// 2^gpu_region_bits tile (src/core/kernel.cu:195-235) and launches one
+// kernel per group.  This planner keeps that idea -- one HBM round trip
+// ("pass") applies a whole batch of gates to a tile held on chip -- but
+//   * lets gates that commute move past each other (two gates commute when
+//     every index bit they share is acted on diagonally by both: controls
+//     always are, a target is iff the matrix is diagonal);
+//   * treats diagonal gates as tile-independent (they never pair amplitudes,
+//     so any pass can apply them whatever its tile bits are);
+//   * picks any set of tile bits (not one contiguous window), always keeping
+//     the low `low_bits` index bits so every tile is a set of contiguous
+//     128-byte runs;
+//   * optionally fuses adjacent gates on the same target and controls into
+//     one matrix (product formed in FP64).
+// Inside a pass, gates are split into register phases of the warp-tile
+// kernel (kernels.cuh): each phase holds the gates whose targets are
+// register bits of one of the three layouts C, B, A.
+#include <algorithm>
+#include <cstring>
+
+#include "hgm_internal.h"
+
+namespace hgm {
+
+namespace {
+
+struct SOp {
+    int target;
+    uint64_t cmask, cval;
+    cplx m[4];
+    MatClass mc;
+    uint64_t nd() const { return mc == MC_DIAG ? 0 : (uint64_t(1) << target); }
+    uint64_t dg() const { return cmask | (mc == MC_DIAG ? (uint64_t(1) << target) : 0); }
+    uint64_t sup() const { return cmask | (uint64_t(1) << target); }
+};
+
+inline bool conflicts(const SOp &o, uint64_t b_nd, uint64_t b_d) {
+    return (o.nd() & (b_nd | b_d)) || (o.dg() & b_nd);
+}
+
+void matmul2(const cplx a[4], const cplx b[4], cplx out[4]) {  // out = a * b
+    cplx r[4] = {a[0] * b[0] + a[1] * b[2], a[0] * b[1] + a[1] * b[3], a[2] * b[0] + a[3] * b[2],
+                 a[2] * b[1] + a[3] * b[3]};
+    for (int k = 0; k < 4; k++) out[k] = r[k];
+}
+
+std::vector<SOp> fuse_ops(const std::vector<Op> &ops, bool fuse) {
+    std::vector<SOp> out;
+    out.reserve(ops.size());
+    int64_t last_touch[64];
+    for (int b = 0; b < 64; b++) last_touch[b] = -1;
+    for (const Op &op : ops) {
+        SOp s;
+        s.target = op.target;
+        s.cmask = op.cmask;
+        s.cval = op.cval;
+        for (int k = 0; k < 4; k++) s.m[k] = op.m[k];
+        s.mc = classify(s.m);
+        if (fuse) {
+            int64_t y = last_touch[op.target];
+            if (y >= 0 && out[y].target == s.target && out[y].cmask == s.cmask && out[y].cval == s.cval) {
+                bool adjacent = true;
+                uint64_t sup = s.sup();
+                while (sup) {
+                    int b = __builtin_ctzll(sup);
+                    sup &= sup - 1;
+                    if (last_touch[b] != y) {
+                        adjacent = false;
+                        break;
+                    }
+                }
+                if (adjacent) {
+                    matmul2(s.m, out[y].m, out[y].m);
+                    out[y].mc = classify(out[y].m);
+                    continue;
+                }
+            }
+        }
+        out.push_back(s);
+        uint64_t sup = s.sup();
+        while (sup) {
+            int b = __builtin_ctzll(sup);
+            sup &= sup - 1;
+            last_touch[b] = (int64_t)out.size() - 1;
+        }
+    }
+    return out;
+}
+
+// Register-bit ranges of the three layouts of a CTA tile with W warp bits:
+//   C: lanes = local 0..4,  regs = local 5..9,   warps = local 10..
+//   B: regs  = local 0..4,  lanes = local 5..9,  warps = local 10..
+//   A: lanes = local 0..4,  warps = local 5..4+W, regs = local 5+W..9+W
+struct LayoutRanges {
+    int ls, rs, ws;
+};
+LayoutRanges ranges(int layout, int W) {
+    switch (layout) {
+        case LAYOUT_C: return {0, 5, 10};
+        case LAYOUT_B: return {5, 0, 10};
+        default: return {0, 5 + W, 5};
+    }
+}
+inline bool in_regs(int layout, int W, int loc) {
+    LayoutRanges r = ranges(layout, W);
+    return loc >= r.rs && loc < r.rs + 5;
+}
+
+template <typename Real>
+DevOp<Real> encode(const SOp &o, int layout, int W, const int loc_of[64], uint64_t tile_mask) {
+    DevOp<Real> d;
+    memset(&d, 0, sizeof d);
+    LayoutRanges r = ranges(layout, W);
+    auto thr_index = [&](int loc) -> int {
+        if (loc >= r.ls && loc < r.ls + 5) return loc - r.ls;
+        return 5 + (loc - r.ws);
+    };
+    uint64_t cm = o.cmask;
+    while (cm) {
+        int g = __builtin_ctzll(cm);
+        cm &= cm - 1;
+        uint32_t v = (o.cval >> g) & 1;
+        if (!((tile_mask >> g) & 1)) {
+            d.cm_glob |= uint64_t(1) << g;
+            d.cv_glob |= uint64_t(v) << g;
+            continue;
+        }
+        int loc = loc_of[g];
+        if (loc >= r.rs && loc < r.rs + 5) {
+            d.cm_reg |= 1u << (loc - r.rs);
+            d.cv_reg |= v << (loc - r.rs);
+        } else {
+            int t = thr_index(loc);
+            d.cm_thr |= 1u << t;
+            d.cv_thr |= v << t;
+        }
+    }
+    const cplx *m = o.m;
+    bool all_real = m[0].imag() == 0 && m[1].imag() == 0 && m[2].imag() == 0 && m[3].imag() == 0;
+    switch (o.mc) {
+        case MC_DENSE: d.kind = all_real ? K_REAL : K_DENSE; break;
+        case MC_DIAG: d.kind = (m[0] == 1.0) ? K_PHASE : K_DIAG; break;
+        default: d.kind = (m[1] == 1.0 && m[2] == 1.0) ? K_SWAP : K_ANTI; break;
+    }
+    int g = o.target;
+    if (!((tile_mask >> g) & 1)) {
+        d.tpos = TPOS_GLOBAL + g;  // diagonal gates only
+    } else {
+        int loc = loc_of[g];
+        if (loc >= r.rs && loc < r.rs + 5) d.tpos = loc - r.rs;
+        else d.tpos = TPOS_THREAD + thr_index(loc);
+    }
+    for (int k = 0; k < 4; k++) {
+        d.m[2 * k] = (Real)m[k].real();
+        d.m[2 * k + 1] = (Real)m[k].imag();
+    }
+    return d;
+}
+
+template <typename Real>
+SmallOp<Real> encode_small(const SOp &o) {
+    SmallOp<Real> s;
+    memset(&s, 0, sizeof s);
+    s.target = o.target;
+    s.kind = o.mc;
+    s.cmask = (uint32_t)o.cmask;
+    s.cval = (uint32_t)o.cval;
+    for (int k = 0; k < 4; k++) {
+        s.m[2 * k] = (Real)o.m[k].real();
+        s.m[2 * k + 1] = (Real)o.m[k].imag();
+    }
+    return s;
+}
+
+// Doubly linked list over op indices (scheduling removes from the middle).
+struct OpList {
+    std::vector<int> nxt, prv;
+    int head = -1;
+    explicit OpList(int n) : nxt(n), prv(n) {
+        for (int i = 0; i < n; i++) {
+            nxt[i] = i + 1 < n ? i + 1 : -1;
+            prv[i] = i - 1;
+        }
+        head = n ? 0 : -1;
+    }
+    void remove(int i) {
+        if (prv[i] >= 0) nxt[prv[i]] = nxt[i];
+        else head = nxt[i];
+        if (nxt[i] >= 0) prv[nxt[i]] = prv[i];
+    }
+};
+
+template <typename Real>
+int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan *plan) {
+    const int W = plan->warp_bits;
+    const int K = 10 + W;
+    const int L = std::min(o.low_bits, K);
+    const int window = o.window > 0 ? o.window : 4096;
+    const uint64_t all_bits = (n >= 64) ? ~uint64_t(0) : ((uint64_t(1) << n) - 1);
+    std::vector<DevOp<Real>> dev_ops;
+    dev_ops.reserve(ops.size());
+
+    OpList list((int)ops.size());
+    std::vector<int> pass_ops;
+    int pass_index = 0;
+    while (list.head >= 0) {
+        uint64_t tmask = (uint64_t(1) << L) - 1;
+        int tcount = L;
+        uint64_t b_nd = 0, b_d = 0;
+        pass_ops.clear();
+        int since_take = 0;
+        for (int i = list.head; i >= 0;) {
+            const SOp &op = ops[i];
+            int nexti = list.nxt[i];
+            bool take = false;
+            if (!conflicts(op, b_nd, b_d)) {
+                uint64_t tb = uint64_t(1) << op.target;
+                if (op.mc == MC_DIAG || (tmask & tb)) take = true;
+                else if (tcount < K) {
+                    tmask |= tb;
+                    tcount++;
+                    take = true;
+                }
+            }
+            if (take) {
+                pass_ops.push_back(i);
+                list.remove(i);
+                since_take = 0;
+            } else {
+                b_nd |= op.nd();
+                b_d |= op.dg();
+                if (++since_take > window) break;
+                if ((b_nd & all_bits) == all_bits) break;
+            }
+            i = nexti;
+        }
+        if (pass_ops.empty()) return fail(HGM_ERR_INVALID, "planner made no progress");
+        // fill the tile up to K bits with the lowest unused index bits
+        for (int g = 0; tcount < K && g < n; g++) {
+            if (!((tmask >> g) & 1)) {
+                tmask |= uint64_t(1) << g;
+                tcount++;
+            }
+        }
+        // local positions: low bits fixed, then by first dense use into
+        // C-register slots, A-only slots, then B-only (lane) slots.
+        std::vector<int> order;
+        uint64_t placed = (uint64_t(1) << L) - 1;
+        for (int idx : pass_ops) {
+            const SOp &op = ops[idx];
+            uint64_t tb = uint64_t(1) << op.target;
+            if (op.mc != MC_DIAG && !(placed & tb)) {
+                placed |= tb;
+                order.push_back(op.target);
+            }
+        }
+        for (int g = 0; g < n; g++)
+            if (((tmask >> g) & 1) && !((placed >> g) & 1)) {
+                placed |= uint64_t(1) << g;
+                order.push_back(g);
+            }
+        std::vector<int> slots;
+        for (int q = 5; q < 10; q++) slots.push_back(q);
+        for (int q = 10; q < 10 + W; q++) slots.push_back(q);
+        for (int q = L; q < 5; q++) slots.push_back(q);
+        int loc_of[64];
+        for (int g = 0; g < 64; g++) loc_of[g] = -1;
+        PassArgs pa;
+        memset(&pa, 0, sizeof pa);
+        pa.n = n;
+        pa.k = K;
+        for (int g = 0; g < L; g++) {
+            loc_of[g] = g;
+            pa.tb[g] = (int8_t)g;
+        }
+        for (size_t j = 0; j < order.size(); j++) {
+            loc_of[order[j]] = slots[j];
+            pa.tb[slots[j]] = (int8_t)order[j];
+        }
+        pa.tile_mask = tmask;
+
+        // register phases
+        pa.phase_begin = (int)plan->phases.size();
+        std::vector<int> pending = pass_ops;
+        int cur = -1;
+        const int layouts[3] = {LAYOUT_C, LAYOUT_A, LAYOUT_B};
+        const int n_layouts = W > 0 ? 3 : 2;
+        std::vector<int> taken, rest;
+        while (!pending.empty()) {
+            int best = -1, best_count = -1;
+            for (int li = 0; li < 3; li++) {
+                int lay = layouts[li];
+                if (lay == LAYOUT_A && W == 0) continue;
+                uint64_t bn = 0, bd = 0;
+                int count = 0;
+                for (int idx : pending) {
+                    const SOp &op = ops[idx];
+                    bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(lay, W, loc_of[op.target]));
+                    if (ok) count++;
+                    else {
+                        bn |= op.nd();
+                        bd |= op.dg();
+                    }
+                }
+                if (count > best_count || (count == best_count && lay == cur)) {
+                    best = lay;
+                    best_count = count;
+                }
+            }
+            (void)n_layouts;
+            taken.clear();
+            rest.clear();
+            uint64_t bn = 0, bd = 0;
+            for (int idx : pending) {
+                const SOp &op = ops[idx];
+                bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(best, W, loc_of[op.target]));
+                if (ok) taken.push_back(idx);
+                else {
+                    rest.push_back(idx);
+                    bn |= op.nd();
+                    bd |= op.dg();
+                }
+            }
+            if (taken.empty()) return fail(HGM_ERR_INVALID, "phase scheduling made no progress");
+            DevPhase ph;
+            ph.layout = best;
+            ph.op_begin = (int)dev_ops.size();
+            for (int idx : taken) dev_ops.push_back(encode<Real>(ops[idx], best, W, loc_of, tmask));
+            ph.op_end = (int)dev_ops.size();
+            int prev = cur < 0 ? (best == LAYOUT_A ? LAYOUT_A : LAYOUT_C) : cur;
+            ph.xwarp = (prev != best) && (prev == LAYOUT_A || best == LAYOUT_A) ? 1 : 0;
+            if (prev != best) plan->n_transposes++;
+            plan->phases.push_back(ph);
+            cur = best;
+            pending.swap(rest);
+        }
+        pa.phase_end = (int)plan->phases.size();
+        const DevPhase &first = plan->phases[pa.phase_begin];
+        pa.load_layout = first.layout == LAYOUT_A ? LAYOUT_A : LAYOUT_C;
+        pa.store_layout = cur == LAYOUT_A ? LAYOUT_A : LAYOUT_C;
+        if (cur == LAYOUT_B) plan->n_transposes++;
+        plan->passes.push_back(pa);
+        pass_index++;
+    }
+    plan->ops_bytes.resize(dev_ops.size() * sizeof(DevOp<Real>));
+    if (!dev_ops.empty()) memcpy(plan->ops_bytes.data(), dev_ops.data(), plan->ops_bytes.size());
+    return HGM_OK;
+}
+
+template <typename Real>
+int build_small(const std::vector<SOp> &ops, Plan *plan) {
+    std::vector<SmallOp<Real>> so;
+    so.reserve(ops.size());
+    for (const SOp &o : ops) so.push_back(encode_small<Real>(o));
+    plan->ops_bytes.resize(so.size() * sizeof(SmallOp<Real>));
+    if (!so.empty()) memcpy(plan->ops_bytes.data(), so.data(), plan->ops_bytes.size());
+    plan->n_small_ops = (int64_t)so.size();
+    return HGM_OK;
+}
+
+}  // namespace
+
+int build_plan(const std::vector<Op> &ops, int n, const hgm_plan_opts &opts, Plan *plan) {
+    if (n < 1 || n > 34) return fail(HGM_ERR_UNSUPPORTED, "qubits=%d outside 1..34", n);
+    for (const Op &op : ops) {
+        if (op.target < 0 || op.target >= n) return fail(HGM_ERR_INVALID, "target bit %d outside 0..%d", op.target, n - 1);
+        if (n < 64 && (op.cmask >> n)) return fail(HGM_ERR_INVALID, "control mask beyond %d qubits", n);
+        if (op.cmask & (uint64_t(1) << op.target)) return fail(HGM_ERR_INVALID, "target is also a control");
+    }
+    plan->precision = opts.precision;
+    plan->qubits = n;
+    plan->renorm_every = opts.precision == HGM_F32 ? opts.renorm_every : 0;
+    std::vector<SOp> sops = fuse_ops(ops, opts.fuse != 0);
+    plan->n_ops = (int64_t)sops.size();
+    if (n < 10) {
+        plan->small = true;
+        plan->warp_bits = 0;
+        return opts.precision == HGM_F64 ? build_small<double>(sops, plan) : build_small<float>(sops, plan);
+    }
+    int W = opts.warp_bits;
+    if (W < 0) W = opts.precision == HGM_F64 ? 2 : 2;
+    W = std::min(W, 3);
+    W = std::min(W, n - 10);
+    plan->warp_bits = W;
+    hgm_plan_opts o = opts;
+    if (o.low_bits < 0) o.low_bits = opts.precision == HGM_F64 ? 3 : 4;
+    o.low_bits = std::max(0, std::min(o.low_bits, 5));
+    return opts.precision == HGM_F64 ? build_tiled<double>(sops, n, o, plan) : build_tiled<float>(sops, n, o, plan);
+}
+
+}  // namespace hgm

@@ -1,0 +1,284 @@
+"""Python face of the engine: circuits, plans, device states and a DGM mirror.
+
+Everything here calls libhgm_b200.so through ctypes (_lib.py); there is no
+Python or CPU compute path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import HGM_F32, HGM_F64, PlanOpts, check, lib
+
+PREC = {"f64": HGM_F64, "f32": HGM_F32, HGM_F64: HGM_F64, HGM_F32: HGM_F32}
+NP_DTYPE = {HGM_F64: np.complex128, HGM_F32: np.complex64}
+
+_initialised = False
+
+
+def init(device: int = 0):
+    """Creates the CUDA context on `device` (setDevice, src/core/kernel.cu:31-33)."""
+    global _initialised
+    if not _initialised:
+        check(lib.hgm_init(device))
+        _initialised = True
+
+
+def _m8(m) -> "C.Array":
+    m = np.asarray(m, dtype=np.complex128).reshape(4)
+    buf = (C.c_double * 8)()
+    for k in range(4):
+        buf[2 * k] = float(m[k].real)
+        buf[2 * k + 1] = float(m[k].imag)
+    return buf
+
+
+class Circuit:
+    """Compiled op list built with the reference's circuit language.
+
+    ``add_gate`` = Gates::addGate (src/core/gates.cpp:42-60),
+    ``set_function`` = DGM::setFunction (src/core/dgm_parser.cpp:29-66).
+    """
+
+    def __init__(self):
+        self.h = lib.hgm_circuit_new()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.hgm_circuit_free(self.h)
+            self.h = None
+
+    def add_gate(self, name: str, m) -> bool:
+        rc = lib.hgm_circuit_add_gate(self.h, name.encode(), _m8(m))
+        if rc < 0:
+            raise _lib.HgmError(-rc, _lib.last_error())
+        return rc == 1
+
+    def set_function(self, steps, iterations: int = 1, reset: bool = True):
+        if not isinstance(steps, str):
+            steps = ";".join(steps)
+        check(lib.hgm_circuit_set_function(self.h, steps.encode(), iterations, 1 if reset else 0))
+        return self
+
+    def append_op(self, target, cmask, cval, m):
+        check(lib.hgm_circuit_append_op(self.h, target, cmask, cval, _m8(m)))
+
+    @property
+    def qubits(self) -> int:
+        return lib.hgm_circuit_qubits(self.h)
+
+    def __len__(self):
+        return lib.hgm_circuit_num_ops(self.h)
+
+    def ops(self):
+        n = len(self)
+        t = np.empty(n, np.int32)
+        cm = np.empty(n, np.int64)
+        cv = np.empty(n, np.int64)
+        m = np.empty(8 * n, np.float64)
+        if n:
+            check(lib.hgm_circuit_get_ops(self.h, t.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          cm.ctypes.data_as(C.POINTER(C.c_int64)),
+                                          cv.ctypes.data_as(C.POINTER(C.c_int64)),
+                                          m.ctypes.data_as(C.POINTER(C.c_double))))
+        mm = m.reshape(n, 4, 2)
+        return t, cm, cv, mm[..., 0] + 1j * mm[..., 1]
+
+    def ref_pts(self, precision="f64"):
+        """NULL-terminated PT** in the reference's struct layout."""
+        p = lib.hgm_circuit_ref_pts(self.h, PREC[precision])
+        if not p:
+            raise _lib.HgmError(1, _lib.last_error())
+        return p
+
+
+def plan_opts(precision="f64", **kw) -> PlanOpts:
+    o = PlanOpts()
+    lib.hgm_plan_default_opts(C.byref(o), PREC[precision])
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Plan:
+    def __init__(self, circuit: Circuit, qubits: int, precision="f64", **kw):
+        self.h = C.c_void_p()
+        self.precision = PREC[precision]
+        self.qubits = qubits
+        check(lib.hgm_plan_create(circuit.h, qubits, C.byref(plan_opts(precision, **kw)), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.hgm_plan_free(self.h)
+            self.h = None
+
+    def stats(self) -> dict:
+        v = [C.c_int64() for _ in range(4)]
+        check(lib.hgm_plan_stats(self.h, *[C.byref(x) for x in v]))
+        return dict(ops=v[0].value, passes=v[1].value, phases=v[2].value, transposes=v[3].value)
+
+
+class State:
+    """A device-resident state vector."""
+
+    def __init__(self, qubits: int, precision="f64"):
+        init()
+        self.qubits = qubits
+        self.precision = PREC[precision]
+        self.h = C.c_void_p()
+        check(lib.hgm_state_create(qubits, self.precision, C.byref(self.h)))
+
+    def free(self):
+        if getattr(self, "h", None):
+            lib.hgm_state_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.free()
+
+    @property
+    def nbytes(self):
+        return (1 << self.qubits) * (16 if self.precision == HGM_F64 else 8)
+
+    def set_basis(self, index: int):
+        check(lib.hgm_state_set_basis(self.h, index))
+        return self
+
+    def upload(self, host):
+        arr = np.ascontiguousarray(np.asarray(host, dtype=NP_DTYPE[self.precision]))
+        check(lib.hgm_state_upload(self.h, arr.ctypes.data, arr.nbytes))
+        return self
+
+    def download(self, out=None):
+        if out is None:
+            out = np.empty(1 << self.qubits, dtype=NP_DTYPE[self.precision])
+        check(lib.hgm_state_download(self.h, out.ctypes.data, out.nbytes))
+        return out
+
+    def execute(self, plan: Plan, iterations: int = 1, stream=None):
+        check(lib.hgm_execute(self.h, plan.h, iterations, stream))
+        return self
+
+    def norm(self) -> float:
+        v = C.c_double()
+        check(lib.hgm_norm(self.h, C.byref(v)))
+        return v.value
+
+    def prob_one(self, bit: int) -> float:
+        v = C.c_double()
+        check(lib.hgm_prob_one(self.h, bit, C.byref(v)))
+        return v.value
+
+    def measure_qubit(self, qubit: int, sample: float):
+        o, p = C.c_int(), C.c_double()
+        check(lib.hgm_measure_qubit(self.h, qubit, sample, C.byref(o), C.byref(p)))
+        return o.value, p.value
+
+    def marginal_argmax(self, mask: int):
+        a, p = C.c_int64(), C.c_double()
+        check(lib.hgm_marginal_argmax(self.h, mask, C.byref(a), C.byref(p)))
+        return a.value, p.value
+
+    def inner(self, other: "State"):
+        re, im = C.c_double(), C.c_double()
+        check(lib.hgm_inner(self.h, other.h, C.byref(re), C.byref(im)))
+        return complex(re.value, im.value)
+
+    def max_abs_diff(self, other: "State") -> float:
+        v = C.c_double()
+        check(lib.hgm_max_abs_diff(self.h, other.h, C.byref(v)))
+        return v.value
+
+    def scale(self, f: float):
+        check(lib.hgm_scale(self.h, f))
+
+
+def synchronize():
+    check(lib.hgm_synchronize())
+
+
+def kernel_launches() -> int:
+    return lib.hgm_kernel_launches()
+
+
+class Timer:
+    """CUDA events around the work queued on the library stream."""
+
+    def __enter__(self):
+        check(lib.hgm_timer_start())
+        return self
+
+    def __exit__(self, *a):
+        ms = C.c_double()
+        check(lib.hgm_timer_stop(C.byref(ms)))
+        self.ms = ms.value
+
+
+# ---------------------------------------------------------------------------
+# DGM mirror (include/core/dgm.h:65-163) with a device-resident state
+# ---------------------------------------------------------------------------
+
+T_CPU, T_PAR_CPU, T_GPU, T_HYBRID = 0, 1, 2, 3
+
+
+@dataclass
+class DGM:
+    """The reference's DGM facade on the B200 engine.
+
+    Same fields and call sequence as include/core/dgm.h:65-163 (qubits,
+    exec_type, tuning fields, allocateMemory, setMemoryValue, setFunction,
+    execute, measure), with the state kept on the device.  Only exec_type
+    t_GPU is provided; the tuning fields are validated like
+    DGM::validateTuning (src/core/dgm_core.cpp:177-241).
+    """
+
+    qubits: int = 0
+    exec_type: int = T_GPU
+    precision: str = "f64"
+    gpu_count: int = 1
+    gpu_region_bits: int = 8
+    gpu_coalesced_bits: int = 4
+    block_size: int = 64
+    repeat_count: int = 2
+    circuit: Circuit = field(default_factory=Circuit)
+    state: State | None = None
+
+    def allocateMemory(self):
+        self.state = State(self.qubits, self.precision)
+        self.state.set_basis(0)
+
+    def setMemoryValue(self, pos: int):
+        self.state.set_basis(pos)
+
+    def setFunction(self, steps, iterations=1, reset=True):
+        self.circuit.set_function(steps, iterations, reset)
+
+    def validateTuning(self):
+        if self.exec_type != T_GPU:
+            raise ValueError(f"exec_type {self.exec_type} is not provided by the B200 engine (t_GPU only)")
+        self.gpu_region_bits = min(self.gpu_region_bits, self.qubits)
+        if 2 * self.block_size * self.repeat_count != (1 << self.gpu_region_bits):
+            raise ValueError("2*block_size*repeat_count must equal 2^gpu_region_bits")
+        if self.gpu_region_bits < self.gpu_coalesced_bits:
+            raise ValueError("gpu_region_bits must be >= gpu_coalesced_bits")
+
+    def execute(self, iterations=1):
+        self.validateTuning()
+        plan = Plan(self.circuit, self.qubits, self.precision)
+        self.state.execute(plan, iterations)
+        return self.state
+
+    def executeFunction(self, steps, iterations=1):
+        self.setFunction(steps)
+        return self.execute(iterations)
+
+    def measure(self, qubit_pos: int, sample: float) -> int:
+        """DGM::measure(int) with the uniform sample supplied by the caller."""
+        outcome, _ = self.state.measure_qubit(qubit_pos, sample)
+        return outcome
+
+    def host_state(self):
+        return self.state.download()
