@@ -100,6 +100,13 @@ void hgm_plan_free(hgm_plan *p);
 /* Plan statistics: ops after fusion, passes, phases, transposes. */
 int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes);
 
+/* Read-only view of a plan's host-side encoding (for inspection and the
+ * CPU emulation test): per-pass kernel arguments (struct PassArgs), register
+ * phases (struct DevPhase) and encoded gates (DevOp or SmallOp records), as
+ * laid out in simulador_quantico_b200/csrc/hgm_internal.h. */
+int hgm_plan_export(const hgm_plan *p, const void **passes, int64_t *n_passes, const void **phases,
+                    int64_t *n_phases, const void **ops, int64_t *ops_bytes, int *warp_bits, int *small);
+
 /* ---- device-resident states -------------------------------------------- */
 
 int hgm_state_create(int qubits, int precision, hgm_state **out);
@@ -137,6 +144,28 @@ int hgm_inner(hgm_state *a, hgm_state *b, double *re, double *im);
 int hgm_max_abs_diff(hgm_state *a, hgm_state *b, double *out);
 /* Multiplies every amplitude by `scale`. */
 int hgm_scale(hgm_state *s, double scale);
+
+/* ---- batched mode --------------------------------------------------------- */
+/* Many independent circuits of uneven size run by one persistent kernel that
+ * a CUDA graph replays: hgm_batch_add the circuits, hgm_batch_finalize
+ * (plans every circuit for the same register tile of 2^(5+R+warp_bits)
+ * amplitudes, lays the states out in one device arena, captures the graph),
+ * then hgm_batch_run as often as needed.  Each run resets every state to its
+ * initial basis index and applies its circuit. */
+
+typedef struct hgm_batch hgm_batch;
+int hgm_batch_create(int precision, int warp_bits, hgm_batch **out);
+void hgm_batch_free(hgm_batch *b);
+/* Adds a circuit on `qubits` qubits starting from |init_index>; returns its job index. */
+int hgm_batch_add(hgm_batch *b, const hgm_circuit *c, int qubits, int64_t init_index, int *job);
+int hgm_batch_finalize(hgm_batch *b);
+/* Launches the graph on `stream` (0 = library stream); asynchronous. */
+int hgm_batch_run(hgm_batch *b, void *stream);
+/* After a run has completed: HGM_ERR_TIMEOUT if a tile gave up waiting. */
+int hgm_batch_check(hgm_batch *b);
+int hgm_batch_size(const hgm_batch *b, int *jobs, int64_t *tasks, int64_t *items, int64_t *arena_bytes);
+/* A view of one job's state (owned by the batch; hgm_state_free ignores it). */
+hgm_state *hgm_batch_state(hgm_batch *b, int job);
 
 /* ---- timing (CUDA events on the library stream) ------------------------- */
 

@@ -31,7 +31,7 @@ class PlanOpts(C.Structure):
 
 def _load():
     if not ENGINE.exists():
-        raise ImportError(f"{ENGINE} is missing: build it with `python -m simulador_quantico_b200.build`")
+        raise ImportError(f"{ENGINE} is missing: build it with `python simulador_quantico_b200/build.py`")
     L = C.CDLL(str(ENGINE))
     vp, i, i64, d = C.c_void_p, C.c_int, C.c_int64, C.c_double
     P = C.POINTER
@@ -55,6 +55,7 @@ def _load():
         "hgm_plan_create_from_ref_pts": ([vp, i, i, P(PlanOpts), P(vp)], i),
         "hgm_plan_free": ([vp], None),
         "hgm_plan_stats": ([vp, P(i64), P(i64), P(i64), P(i64)], i),
+        "hgm_plan_export": ([vp, P(vp), P(i64), P(vp), P(i64), P(vp), P(i64), P(i), P(i)], i),
         "hgm_state_create": ([i, i, P(vp)], i),
         "hgm_state_free": ([vp], None),
         "hgm_state_qubits": ([vp], i),
@@ -71,6 +72,14 @@ def _load():
         "hgm_inner": ([vp, vp, P(d), P(d)], i),
         "hgm_max_abs_diff": ([vp, vp, P(d)], i),
         "hgm_scale": ([vp, d], i),
+        "hgm_batch_create": ([i, i, P(vp)], i),
+        "hgm_batch_free": ([vp], None),
+        "hgm_batch_add": ([vp, vp, i, i64, P(i)], i),
+        "hgm_batch_finalize": ([vp], i),
+        "hgm_batch_run": ([vp, vp], i),
+        "hgm_batch_check": ([vp], i),
+        "hgm_batch_size": ([vp, P(i), P(i64), P(i64), P(i64)], i),
+        "hgm_batch_state": ([vp, i], vp),
         "hgm_timer_start": ([], i),
         "hgm_timer_stop": ([P(d)], i),
     }
@@ -99,7 +108,7 @@ def load_dropin(prec: str):
     """The reference-ABI library (setDevice / GpuExecutionWrapper / ...)."""
     so = DROPIN[prec]
     if not so.exists():
-        raise ImportError(f"{so} is missing: build it with `python -m simulador_quantico_b200.build`")
+        raise ImportError(f"{so} is missing: build it with `python simulador_quantico_b200/build.py`")
     L = C.CDLL(str(so))
     L.setDevice.argtypes = [C.c_int]
     L.setDevice.restype = C.c_bool

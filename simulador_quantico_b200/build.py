@@ -4,8 +4,8 @@
     libhgm_dropin_f32.so    reference GPU-backend symbols, complex float
     libhgm_dropin_f64.so    reference GPU-backend symbols, complex double
 
-Output: simulador_quantico_b200/lib/.  Run ``python -m simulador_quantico_b200.build``
-or call ``build()``; a library is rebuilt when any source or header is newer.
+Output: simulador_quantico_b200/lib/.  Run ``python simulador_quantico_b200/build.py``
+(the package itself imports only once the libraries exist) or call ``build()``; a library is rebuilt when any source or header is newer.
 """
 from __future__ import annotations
 
@@ -24,7 +24,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}", "-ccbin", "g++"]
 
-ENGINE_SRCS = ["circuit.cpp", "planner.cpp", "engine.cpp", "kernels.cu"]
+ENGINE_SRCS = ["circuit.cpp", "planner.cpp", "engine.cpp", "kernels.cu", "batch.cu"]
+# Extra nvcc flags (e.g. -DHGM_MAXREG_F32=128) and an alternative output
+# folder, for building tuning variants side by side.
+EXTRA_FLAGS = os.environ.get("HGM_NVCC_EXTRA", "").split()
 
 
 def _nvcc():
@@ -47,7 +50,8 @@ def _run(cmd, verbose):
     subprocess.run([str(c) for c in cmd], check=True)
 
 
-def build(verbose: bool = False, ptxas_verbose: bool = False) -> None:
+def build(verbose: bool = False, ptxas_verbose: bool = False, lib_dir: Path | None = None) -> None:
+    LIB = Path(lib_dir) if lib_dir else globals()["LIB"]
     LIB.mkdir(parents=True, exist_ok=True)
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     nvcc = _nvcc()
@@ -59,7 +63,7 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> None:
         o = objdir / (src + ".o")
         if _stale(o, [s, *headers]):
             extra = ["-Xptxas", "-v"] if (ptxas_verbose and src.endswith(".cu")) else []
-            _run([nvcc, *ARCH, *NVCC_FLAGS, *extra, "-c", s, "-o", o], verbose)
+            _run([nvcc, *ARCH, *NVCC_FLAGS, *EXTRA_FLAGS, *extra, "-c", s, "-o", o], verbose)
         objs.append(o)
     engine = LIB / "libhgm_b200.so"
     if _stale(engine, objs):
@@ -73,4 +77,5 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> None:
 
 
 if __name__ == "__main__":
-    build(verbose=True, ptxas_verbose="-v" in sys.argv)
+    out = os.environ.get("HGM_LIB_OUT")
+    build(verbose=True, ptxas_verbose="-v" in sys.argv, lib_dir=Path(out) if out else None)

@@ -105,6 +105,21 @@ int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t
     return HGM_OK;
 }
 
+int hgm_plan_export(const hgm_plan *p, const void **passes, int64_t *n_passes, const void **phases,
+                    int64_t *n_phases, const void **ops, int64_t *ops_bytes, int *warp_bits, int *small) {
+    if (!p) return fail(HGM_ERR_INVALID, "null plan");
+    const Plan *pl = reinterpret_cast<const Plan *>(p);
+    if (passes) *passes = pl->passes.data();
+    if (n_passes) *n_passes = (int64_t)pl->passes.size();
+    if (phases) *phases = pl->phases.data();
+    if (n_phases) *n_phases = (int64_t)pl->phases.size();
+    if (ops) *ops = pl->ops_bytes.data();
+    if (ops_bytes) *ops_bytes = (int64_t)pl->ops_bytes.size();
+    if (warp_bits) *warp_bits = pl->warp_bits;
+    if (small) *small = pl->small ? 1 : 0;
+    return HGM_OK;
+}
+
 int hgm_state_create(int qubits, int precision, hgm_state **out) {
     if (!out) return fail(HGM_ERR_INVALID, "null output");
     if (qubits < 1 || qubits > 34) return fail(HGM_ERR_UNSUPPORTED, "qubits=%d outside 1..34", qubits);
@@ -124,7 +139,7 @@ int hgm_state_create(int qubits, int precision, hgm_state **out) {
 
 void hgm_state_free(hgm_state *s) {
     State *st = reinterpret_cast<State *>(s);
-    if (!st) return;
+    if (!st || !st->owned) return;  // views are released by their owner
     if (st->d) cudaFree(st->d);
     delete st;
 }

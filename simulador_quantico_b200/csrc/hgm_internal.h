@@ -50,7 +50,7 @@ struct Circuit {
 // ---- kernel-side encodings (shared with kernels.cuh) ----------------------
 
 // Register-phase layouts of a warp tile (see kernels.cuh).
-enum Layout : int32_t { LAYOUT_C = 0, LAYOUT_B = 1, LAYOUT_A = 2 };
+enum Layout : int32_t { LAYOUT_C = 0, LAYOUT_B = 1, LAYOUT_A = 2, LAYOUT_E = 3 };
 
 enum DevKind : int32_t {
     K_DENSE = 0,   // general 2x2
@@ -61,7 +61,7 @@ enum DevKind : int32_t {
     K_SWAP = 5,    // [[0, 1], [1, 0]]
 };
 
-// Target location codes inside a phase: 0..4 register bit, 8+q thread bit q
+// Target location codes inside a phase: 0..R-1 register bit, 8+q thread bit q
 // (lane bits 0..4, warp bits 5..), 64+g a non-tile index bit g.
 constexpr int TPOS_THREAD = 8;
 constexpr int TPOS_GLOBAL = 64;
@@ -85,7 +85,7 @@ constexpr int MAX_TILE_BITS = 16;
 
 struct PassArgs {
     int32_t n;            // qubits
-    int32_t k;            // tile bits = 10 + W
+    int32_t k;            // tile bits = 5 + R + W
     int32_t phase_begin, phase_end;
     int32_t load_layout, store_layout;
     int32_t flags;        // PASS_* below
@@ -101,7 +101,7 @@ struct PassArgs {
 constexpr int32_t PASS_NORM = 1;
 constexpr int32_t PASS_SCALE = 2;
 
-// Small-state path (n < 10): whole state in one CTA's shared memory, ops
+// Small-state path (n < 5 + R): whole state in one CTA's shared memory, ops
 // applied one at a time.
 template <typename Real>
 struct SmallOp {
@@ -115,7 +115,8 @@ struct Plan {
     int precision = HGM_F64;
     int qubits = 0;
     int warp_bits = 0;
-    bool small = false;               // n < 10: single-CTA shared-memory path
+    int reg_bits = 5;                 // amplitudes per thread = 2^reg_bits
+    bool small = false;               // n < 5 + reg_bits: single-CTA shared-memory path
     std::vector<PassArgs> passes;     // device pointers patched after upload
     std::vector<DevPhase> phases;
     std::vector<unsigned char> ops_bytes;   // DevOp<Real>[] or SmallOp<Real>[]
@@ -129,7 +130,10 @@ struct Plan {
     ~Plan();
 };
 
-int build_plan(const std::vector<Op> &ops, int qubits, const hgm_plan_opts &opts, Plan *plan);
+// force_small: plan the state for the one-CTA shared-memory path even when
+// it is large enough for the register tile (the batched kernel's small tasks).
+int build_plan(const std::vector<Op> &ops, int qubits, const hgm_plan_opts &opts, Plan *plan,
+               bool force_small = false);
 int upload_plan(Plan *plan);
 
 // ---- device state ------------------------------------------------------------
@@ -137,6 +141,7 @@ struct State {
     int qubits = 0;
     int precision = HGM_F64;
     void *d = nullptr;
+    bool owned = true;   // false: a view into memory another object owns (batch arena, server pool)
     int64_t bytes() const { return (int64_t(1) << qubits) * (precision == HGM_F64 ? 16 : 8); }
 };
 

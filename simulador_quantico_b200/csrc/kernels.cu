@@ -82,10 +82,11 @@ static inline int check(const char *what) {
 // pass kernels
 // ---------------------------------------------------------------------------
 
-template <typename Real, int W>
-__global__ void __launch_bounds__(32 << W) pass_kernel(typename V2<Real>::T *__restrict__ state, const PassArgs pa) {
+template <typename Real, int R, int W>
+__global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()))
+    pass_kernel(typename V2<Real>::T *__restrict__ state, const PassArgs pa) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    run_tile<Real, W>(state, pa, blockIdx.x, reinterpret_cast<typename V2<Real>::T *>(smem_raw));
+    run_tile<Real, R, W>(state, pa, blockIdx.x, reinterpret_cast<typename V2<Real>::T *>(smem_raw));
 }
 
 template <typename Real>
@@ -124,35 +125,41 @@ __global__ void __launch_bounds__(256) small_kernel(typename V2<Real>::T *__rest
     for (int i = threadIdx.x; i < N; i += blockDim.x) state[i] = sm[i];
 }
 
-template <typename Real, int W>
+template <typename Real, int R, int W>
 static int setup_pass_kernel() {
     static bool done = false;
     if (done) return HGM_OK;
-    const int smem = (1 << (10 + W)) * (int)sizeof(typename V2<Real>::T);
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<Real, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int smem = (1 << (5 + R + W)) * (int)sizeof(typename V2<Real>::T);
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<Real, R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess && HGM_SMEM_CARVEOUT >= 0)
+        e = cudaFuncSetAttribute(pass_kernel<Real, R, W>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 HGM_SMEM_CARVEOUT);
     if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
     done = true;
     return HGM_OK;
 }
 
-template <typename Real, int W>
+template <typename Real, int R, int W>
 static int launch_pass(void *state, const PassArgs &pa, cudaStream_t st) {
-    int rc = setup_pass_kernel<Real, W>();
+    int rc = setup_pass_kernel<Real, R, W>();
     if (rc) return rc;
     const uint64_t tiles = 1ull << (pa.n - pa.k);
-    const int smem = (1 << (10 + W)) * (int)sizeof(typename V2<Real>::T);
-    pass_kernel<Real, W><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<typename V2<Real>::T *>(state), pa);
+    const int smem = (1 << (5 + R + W)) * (int)sizeof(typename V2<Real>::T);
+    pass_kernel<Real, R, W><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<typename V2<Real>::T *>(state),
+                                                                    pa);
     count_launch();
     return HGM_OK;
 }
 
+// FP64 tiles hold 16 amplitudes a thread (R = 4), FP32 tiles 32 (R = 5).
 template <typename Real>
 static int launch_pass_w(int W, void *state, const PassArgs &pa, cudaStream_t st) {
+    constexpr int R = sizeof(Real) == 8 ? 4 : 5;
     switch (W) {
-        case 0: return launch_pass<Real, 0>(state, pa, st);
-        case 1: return launch_pass<Real, 1>(state, pa, st);
-        case 2: return launch_pass<Real, 2>(state, pa, st);
-        default: return launch_pass<Real, 3>(state, pa, st);
+        case 0: return launch_pass<Real, R, 0>(state, pa, st);
+        case 1: return launch_pass<Real, R, 1>(state, pa, st);
+        case 2: return launch_pass<Real, R, 2>(state, pa, st);
+        default: return launch_pass<Real, R, 3>(state, pa, st);
     }
 }
 

@@ -14,9 +14,9 @@
 //     128-byte runs;
 //   * optionally fuses adjacent gates on the same target and controls into
 //     one matrix (product formed in FP64).
-// Inside a pass, gates are split into register phases of the warp-tile
+// Inside a pass, gates are split into register phases of the register-tile
 // kernel (kernels.cuh): each phase holds the gates whose targets are
-// register bits of one of the three layouts C, B, A.
+// register bits of one of its layouts (C, B, A and, for FP64 tiles, E).
 #include <algorithm>
 #include <cstring>
 
@@ -89,34 +89,43 @@ std::vector<SOp> fuse_ops(const std::vector<Op> &ops, bool fuse) {
     return out;
 }
 
-// Register-bit ranges of the three layouts of a CTA tile with W warp bits:
-//   C: lanes = local 0..4,  regs = local 5..9,   warps = local 10..
-//   B: regs  = local 0..4,  lanes = local 5..9,  warps = local 10..
-//   A: lanes = local 0..4,  warps = local 5..4+W, regs = local 5+W..9+W
-struct LayoutRanges {
-    int ls, rs, ws;
+// Role of local tile bit q in a layout of the register tile (kernels.cuh):
+//   C: lanes = local 0..4,   regs = local 5..4+R,  warps = local 5+R..
+//   B: regs  = local 0..R-1, lanes = local R..R+4, warps = local 5+R..
+//   E: (R = 4) lanes = local 0..3 and 8, regs = local 4..7, warps = local 9..
+//   A: lanes = local 0..4,   warps = local 5..4+W, regs = local 5+W..4+W+R
+enum RoleKind { ROLE_LANE = 0, ROLE_REG = 1, ROLE_WARP = 2 };
+struct Role {
+    int kind, idx;
 };
-LayoutRanges ranges(int layout, int W) {
+Role role(int layout, int R, int W, int q) {
     switch (layout) {
-        case LAYOUT_C: return {0, 5, 10};
-        case LAYOUT_B: return {5, 0, 10};
-        default: return {0, 5 + W, 5};
+        case LAYOUT_C:
+            if (q < 5) return {ROLE_LANE, q};
+            if (q < 5 + R) return {ROLE_REG, q - 5};
+            return {ROLE_WARP, q - 5 - R};
+        case LAYOUT_B:
+            if (q < R) return {ROLE_REG, q};
+            if (q < R + 5) return {ROLE_LANE, q - R};
+            return {ROLE_WARP, q - 5 - R};
+        case LAYOUT_E:
+            if (q < 4) return {ROLE_LANE, q};
+            if (q < 8) return {ROLE_REG, q - 4};
+            if (q == 8) return {ROLE_LANE, 4};
+            return {ROLE_WARP, q - 9};
+        default:
+            if (q < 5) return {ROLE_LANE, q};
+            if (q < 5 + W) return {ROLE_WARP, q - 5};
+            return {ROLE_REG, q - 5 - W};
     }
 }
-inline bool in_regs(int layout, int W, int loc) {
-    LayoutRanges r = ranges(layout, W);
-    return loc >= r.rs && loc < r.rs + 5;
-}
+inline bool in_regs(int layout, int R, int W, int loc) { return role(layout, R, W, loc).kind == ROLE_REG; }
 
 template <typename Real>
-DevOp<Real> encode(const SOp &o, int layout, int W, const int loc_of[64], uint64_t tile_mask) {
+DevOp<Real> encode(const SOp &o, int layout, int R, int W, const int loc_of[64], uint64_t tile_mask) {
     DevOp<Real> d;
     memset(&d, 0, sizeof d);
-    LayoutRanges r = ranges(layout, W);
-    auto thr_index = [&](int loc) -> int {
-        if (loc >= r.ls && loc < r.ls + 5) return loc - r.ls;
-        return 5 + (loc - r.ws);
-    };
+    auto thr_index = [&](const Role &rl) -> int { return rl.kind == ROLE_LANE ? rl.idx : 5 + rl.idx; };
     uint64_t cm = o.cmask;
     while (cm) {
         int g = __builtin_ctzll(cm);
@@ -127,12 +136,12 @@ DevOp<Real> encode(const SOp &o, int layout, int W, const int loc_of[64], uint64
             d.cv_glob |= uint64_t(v) << g;
             continue;
         }
-        int loc = loc_of[g];
-        if (loc >= r.rs && loc < r.rs + 5) {
-            d.cm_reg |= 1u << (loc - r.rs);
-            d.cv_reg |= v << (loc - r.rs);
+        Role rl = role(layout, R, W, loc_of[g]);
+        if (rl.kind == ROLE_REG) {
+            d.cm_reg |= 1u << rl.idx;
+            d.cv_reg |= v << rl.idx;
         } else {
-            int t = thr_index(loc);
+            int t = thr_index(rl);
             d.cm_thr |= 1u << t;
             d.cv_thr |= v << t;
         }
@@ -148,9 +157,8 @@ DevOp<Real> encode(const SOp &o, int layout, int W, const int loc_of[64], uint64
     if (!((tile_mask >> g) & 1)) {
         d.tpos = TPOS_GLOBAL + g;  // diagonal gates only
     } else {
-        int loc = loc_of[g];
-        if (loc >= r.rs && loc < r.rs + 5) d.tpos = loc - r.rs;
-        else d.tpos = TPOS_THREAD + thr_index(loc);
+        Role rl = role(layout, R, W, loc_of[g]);
+        d.tpos = rl.kind == ROLE_REG ? rl.idx : TPOS_THREAD + thr_index(rl);
     }
     for (int k = 0; k < 4; k++) {
         d.m[2 * k] = (Real)m[k].real();
@@ -195,7 +203,8 @@ struct OpList {
 template <typename Real>
 int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan *plan) {
     const int W = plan->warp_bits;
-    const int K = 10 + W;
+    const int R = plan->reg_bits;
+    const int K = 5 + R + W;
     const int L = std::min(o.low_bits, K);
     const int window = o.window > 0 ? o.window : 4096;
     const uint64_t all_bits = (n >= 64) ? ~uint64_t(0) : ((uint64_t(1) << n) - 1);
@@ -261,10 +270,12 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
                 placed |= uint64_t(1) << g;
                 order.push_back(g);
             }
+        // register slots of C, then those only A reaches, then E's, then B's
         std::vector<int> slots;
-        for (int q = 5; q < 10; q++) slots.push_back(q);
-        for (int q = 10; q < 10 + W; q++) slots.push_back(q);
-        for (int q = L; q < 5; q++) slots.push_back(q);
+        for (int q = 5; q < 5 + R; q++) slots.push_back(q);
+        for (int q = 5 + R; q < 5 + R + W; q++) slots.push_back(q);
+        if (R == 4 && L <= 4) slots.push_back(4);
+        for (int q = L; q < R; q++) slots.push_back(q);
         int loc_of[64];
         for (int g = 0; g < 64; g++) loc_of[g] = -1;
         PassArgs pa;
@@ -285,19 +296,19 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
         pa.phase_begin = (int)plan->phases.size();
         std::vector<int> pending = pass_ops;
         int cur = -1;
-        const int layouts[3] = {LAYOUT_C, LAYOUT_A, LAYOUT_B};
-        const int n_layouts = W > 0 ? 3 : 2;
+        const int layouts[4] = {LAYOUT_C, LAYOUT_A, LAYOUT_E, LAYOUT_B};
         std::vector<int> taken, rest;
         while (!pending.empty()) {
             int best = -1, best_count = -1;
-            for (int li = 0; li < 3; li++) {
+            for (int li = 0; li < 4; li++) {
                 int lay = layouts[li];
                 if (lay == LAYOUT_A && W == 0) continue;
+                if (lay == LAYOUT_E && R != 4) continue;
                 uint64_t bn = 0, bd = 0;
                 int count = 0;
                 for (int idx : pending) {
                     const SOp &op = ops[idx];
-                    bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(lay, W, loc_of[op.target]));
+                    bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(lay, R, W, loc_of[op.target]));
                     if (ok) count++;
                     else {
                         bn |= op.nd();
@@ -309,13 +320,12 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
                     best_count = count;
                 }
             }
-            (void)n_layouts;
             taken.clear();
             rest.clear();
             uint64_t bn = 0, bd = 0;
             for (int idx : pending) {
                 const SOp &op = ops[idx];
-                bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(best, W, loc_of[op.target]));
+                bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(best, R, W, loc_of[op.target]));
                 if (ok) taken.push_back(idx);
                 else {
                     rest.push_back(idx);
@@ -327,7 +337,7 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
             DevPhase ph;
             ph.layout = best;
             ph.op_begin = (int)dev_ops.size();
-            for (int idx : taken) dev_ops.push_back(encode<Real>(ops[idx], best, W, loc_of, tmask));
+            for (int idx : taken) dev_ops.push_back(encode<Real>(ops[idx], best, R, W, loc_of, tmask));
             ph.op_end = (int)dev_ops.size();
             int prev = cur < 0 ? (best == LAYOUT_A ? LAYOUT_A : LAYOUT_C) : cur;
             ph.xwarp = (prev != best) && (prev == LAYOUT_A || best == LAYOUT_A) ? 1 : 0;
@@ -340,7 +350,7 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
         const DevPhase &first = plan->phases[pa.phase_begin];
         pa.load_layout = first.layout == LAYOUT_A ? LAYOUT_A : LAYOUT_C;
         pa.store_layout = cur == LAYOUT_A ? LAYOUT_A : LAYOUT_C;
-        if (cur == LAYOUT_B) plan->n_transposes++;
+        if (cur == LAYOUT_B || cur == LAYOUT_E) plan->n_transposes++;
         plan->passes.push_back(pa);
         pass_index++;
     }
@@ -362,7 +372,7 @@ int build_small(const std::vector<SOp> &ops, Plan *plan) {
 
 }  // namespace
 
-int build_plan(const std::vector<Op> &ops, int n, const hgm_plan_opts &opts, Plan *plan) {
+int build_plan(const std::vector<Op> &ops, int n, const hgm_plan_opts &opts, Plan *plan, bool force_small) {
     if (n < 1 || n > 34) return fail(HGM_ERR_UNSUPPORTED, "qubits=%d outside 1..34", n);
     for (const Op &op : ops) {
         if (op.target < 0 || op.target >= n) return fail(HGM_ERR_INVALID, "target bit %d outside 0..%d", op.target, n - 1);
@@ -374,15 +384,21 @@ int build_plan(const std::vector<Op> &ops, int n, const hgm_plan_opts &opts, Pla
     plan->renorm_every = opts.precision == HGM_F32 ? opts.renorm_every : 0;
     std::vector<SOp> sops = fuse_ops(ops, opts.fuse != 0);
     plan->n_ops = (int64_t)sops.size();
-    if (n < 10) {
+    // amplitudes per thread: 16 for FP64 (64 data registers), 32 for FP32
+    const int R = opts.precision == HGM_F64 ? 4 : 5;
+    plan->reg_bits = R;
+    if (n < 5 + R || force_small) {
+        if (n > 14) return fail(HGM_ERR_UNSUPPORTED, "the shared-memory path takes at most 14 qubits");
         plan->small = true;
         plan->warp_bits = 0;
         return opts.precision == HGM_F64 ? build_small<double>(sops, plan) : build_small<float>(sops, plan);
     }
+    // Default CTA: 4 warps (tile of 2^11 FP64 / 2^12 FP32 amplitudes), the
+    // fastest size in the pass micro-benchmarks for both precisions.
     int W = opts.warp_bits;
-    if (W < 0) W = opts.precision == HGM_F64 ? 2 : 2;
+    if (W < 0) W = 2;
     W = std::min(W, 3);
-    W = std::min(W, n - 10);
+    W = std::min(W, n - 5 - R);
     plan->warp_bits = W;
     hgm_plan_opts o = opts;
     if (o.low_bits < 0) o.low_bits = opts.precision == HGM_F64 ? 3 : 4;

@@ -118,7 +118,10 @@ class Plan:
     def stats(self) -> dict:
         v = [C.c_int64() for _ in range(4)]
         check(lib.hgm_plan_stats(self.h, *[C.byref(x) for x in v]))
-        return dict(ops=v[0].value, passes=v[1].value, phases=v[2].value, transposes=v[3].value)
+        wb, small = C.c_int(), C.c_int()
+        check(lib.hgm_plan_export(self.h, None, None, None, None, None, None, C.byref(wb), C.byref(small)))
+        return dict(ops=v[0].value, passes=v[1].value, phases=v[2].value, transposes=v[3].value,
+                    warp_bits=wb.value, reg_bits=4 if self.precision == HGM_F64 else 5, small=bool(small.value))
 
 
 class State:
@@ -129,11 +132,20 @@ class State:
         self.qubits = qubits
         self.precision = PREC[precision]
         self.h = C.c_void_p()
+        self.owner = None
         check(lib.hgm_state_create(qubits, self.precision, C.byref(self.h)))
+
+    @classmethod
+    def view(cls, handle, qubits, precision, owner):
+        """A non-owning handle on a state another object (batch, server) owns."""
+        st = cls.__new__(cls)
+        st.qubits, st.precision, st.h, st.owner = qubits, PREC[precision], C.c_void_p(handle), owner
+        return st
 
     def free(self):
         if getattr(self, "h", None):
-            lib.hgm_state_free(self.h)
+            if self.owner is None:
+                lib.hgm_state_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -194,6 +206,50 @@ class State:
 
     def scale(self, f: float):
         check(lib.hgm_scale(self.h, f))
+
+
+class Batch:
+    """Many circuits in one persistent kernel replayed from a CUDA graph (include/hgm_b200.h)."""
+
+    def __init__(self, precision="f32", warp_bits=-1):
+        init()
+        self.precision = PREC[precision]
+        self.h = C.c_void_p()
+        self.qubits = []
+        check(lib.hgm_batch_create(self.precision, warp_bits, C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.hgm_batch_free(self.h)
+            self.h = None
+
+    def add(self, circuit: Circuit, qubits: int, init_index: int = 0) -> int:
+        j = C.c_int()
+        check(lib.hgm_batch_add(self.h, circuit.h, qubits, init_index, C.byref(j)))
+        self.qubits.append(qubits)
+        return j.value
+
+    def finalize(self):
+        check(lib.hgm_batch_finalize(self.h))
+        return self
+
+    def run(self, stream=None):
+        check(lib.hgm_batch_run(self.h, stream))
+        return self
+
+    def check(self):
+        check(lib.hgm_batch_check(self.h))
+
+    def size(self) -> dict:
+        j, t, it, ab = C.c_int(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib.hgm_batch_size(self.h, C.byref(j), C.byref(t), C.byref(it), C.byref(ab)))
+        return dict(jobs=j.value, tasks=t.value, items=it.value, arena_bytes=ab.value)
+
+    def state(self, job: int) -> State:
+        h = lib.hgm_batch_state(self.h, job)
+        if not h:
+            raise _lib.HgmError(1, _lib.last_error())
+        return State.view(h, self.qubits[job], self.precision, owner=self)
 
 
 def synchronize():

@@ -10,6 +10,12 @@ from oracle import cpu
 
 TOL_F64 = 1e-12      # max |amplitude error| vs the FP64 oracle
 TOL_F32 = 2e-5       # max |amplitude error| vs the FP32 oracle (same op order, FP32 rounding)
+REG_BITS = {"f64": 4, "f32": 5}   # amplitudes a thread keeps in registers = 2^R
+
+
+def min_tiled_qubits(prec, warp_bits=0):
+    """Smallest state that runs on the register-tile pass kernel with this many warp bits."""
+    return 5 + REG_BITS[prec] + warp_bits
 
 
 def oracle_state(spec, prec="f64", init=None):

@@ -1,0 +1,163 @@
+"""CPU emulation of a plan's encoded passes (test helper).
+
+Re-executes, with numpy, exactly what the pass kernel (simulador_quantico_b200/
+csrc/kernels.cuh) does with a plan's encoding: per pass, every tile of 2^K
+amplitudes is gathered through the tile-bit map, the register phases run
+with their layout's (lane, warp, register) coordinates and the encoded
+controls, and the tile is scattered back.  Comparing its result with the
+oracle checks the planner and the encoding without a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from simulador_quantico_b200._lib import check, lib
+
+PASS_DT = np.dtype([("n", "<i4"), ("k", "<i4"), ("phase_begin", "<i4"), ("phase_end", "<i4"),
+                    ("load_layout", "<i4"), ("store_layout", "<i4"), ("flags", "<i4"), ("pad", "<i4"),
+                    ("tb", "i1", 16), ("tile_mask", "<u8"), ("phases", "<u8"), ("ops", "<u8"),
+                    ("norm_out", "<u8"), ("scale_in", "<u8")])
+PHASE_DT = np.dtype([("layout", "<i4"), ("op_begin", "<i4"), ("op_end", "<i4"), ("xwarp", "<i4")])
+
+
+def op_dtype(real):
+    fields = [("kind", "<i4"), ("tpos", "<i4"), ("cm_reg", "<u4"), ("cv_reg", "<u4"), ("cm_thr", "<u4"),
+              ("cv_thr", "<u4"), ("cm_glob", "<u8"), ("cv_glob", "<u8"), ("m", real, 8)]
+    dt = np.dtype(fields)
+    size = (dt.itemsize + 15) // 16 * 16
+    return np.dtype({"names": dt.names, "formats": [dt.fields[n][0] for n in dt.names],
+                     "offsets": [dt.fields[n][1] for n in dt.names], "itemsize": size})
+
+
+SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f8", 8)]),
+            "<f4": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f4", 8)])}
+
+K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP = range(6)
+LAYOUT_C, LAYOUT_B, LAYOUT_A, LAYOUT_E = 0, 1, 2, 3
+REG_BITS = {"f64": 4, "f32": 5}
+
+
+def export(plan, precision):
+    p, np_, ph, nph, ops, nb = C.c_void_p(), C.c_int64(), C.c_void_p(), C.c_int64(), C.c_void_p(), C.c_int64()
+    wb, sm = C.c_int(), C.c_int()
+    check(lib.hgm_plan_export(plan.h, C.byref(p), C.byref(np_), C.byref(ph), C.byref(nph), C.byref(ops), C.byref(nb),
+                              C.byref(wb), C.byref(sm)))
+    real = "<f8" if precision == "f64" else "<f4"
+    passes = np.frombuffer(C.string_at(p, np_.value * PASS_DT.itemsize), PASS_DT) if np_.value else np.zeros(0, PASS_DT)
+    phases = np.frombuffer(C.string_at(ph, nph.value * PHASE_DT.itemsize), PHASE_DT) if nph.value else np.zeros(0, PHASE_DT)
+    raw = C.string_at(ops, nb.value) if nb.value else b""
+    odt = SMALL_DT[real] if sm.value else op_dtype(real)
+    opsarr = np.frombuffer(raw, odt) if raw else np.zeros(0, odt)
+    return dict(passes=passes, phases=phases, ops=opsarr, W=wb.value, small=bool(sm.value))
+
+
+def layout_coords(layout, R, W, K):
+    """For every local index j: (lane, warp, reg) in the given layout."""
+    j = np.arange(1 << K)
+    if layout == LAYOUT_C:
+        lane, reg, warp = j & 31, (j >> 5) & ((1 << R) - 1), j >> (5 + R)
+    elif layout == LAYOUT_B:
+        reg, lane, warp = j & ((1 << R) - 1), (j >> R) & 31, j >> (5 + R)
+    elif layout == LAYOUT_E:
+        lane = (j & 15) | (((j >> 8) & 1) << 4)
+        reg, warp = (j >> 4) & 15, j >> 9
+    else:
+        lane, warp, reg = j & 31, (j >> 5) & ((1 << W) - 1), (j >> (5 + W)) & ((1 << R) - 1)
+    return lane, warp, reg
+
+
+def local_of(layout, R, W, lane, warp, reg):
+    if layout == LAYOUT_C:
+        return lane | (reg << 5) | (warp << (5 + R))
+    if layout == LAYOUT_B:
+        return reg | (lane << R) | (warp << (5 + R))
+    if layout == LAYOUT_E:
+        return (lane & 15) | (reg << 4) | ((lane >> 4) << 8) | (warp << 9)
+    return lane | (warp << 5) | (reg << (5 + W))
+
+
+def apply_small(state, ops, n):
+    N = 1 << n
+    idx = np.arange(N)
+    for o in ops:
+        t, cm, cv = int(o["target"]), int(o["cmask"]), int(o["cval"])
+        m = o["m"].astype(np.float64)
+        mm = m[0::2] + 1j * m[1::2]
+        i0 = idx[((idx >> t) & 1) == 0]
+        i0 = i0[(i0 & cm) == cv]
+        i1 = i0 | (1 << t)
+        a0, a1 = state[i0].copy(), state[i1].copy()
+        state[i0] = mm[0] * a0 + mm[1] * a1
+        state[i1] = mm[2] * a0 + mm[3] * a1
+    return state
+
+
+def run(plan, precision, state, iterations=1):
+    e = export(plan, precision)
+    n = plan.qubits
+    state = np.asarray(state, dtype=np.complex128).copy()
+    if e["small"]:
+        for _ in range(iterations):
+            apply_small(state, e["ops"], n)
+        return state
+    W = e["W"]
+    R = REG_BITS[precision]
+    for _ in range(iterations):
+        for pa in e["passes"]:
+            K = int(pa["k"])
+            tb = [int(x) for x in pa["tb"][:K]]
+            tmask = int(pa["tile_mask"])
+            free = [g for g in range(n) if not (tmask >> g) & 1]
+            T = 1 << len(free)
+            tiles = np.arange(T, dtype=np.int64)
+            base = np.zeros(T, dtype=np.int64)
+            for k, g in enumerate(free):
+                base |= ((tiles >> k) & 1) << g
+            j = np.arange(1 << K, dtype=np.int64)
+            scat = np.zeros(1 << K, dtype=np.int64)
+            for q, g in enumerate(tb):
+                scat |= ((j >> q) & 1) << g
+            gidx = base[:, None] | scat[None, :]
+            tile = state[gidx]  # [T, 2^K] by local index
+            for ph in e["phases"][pa["phase_begin"]:pa["phase_end"]]:
+                lay = int(ph["layout"])
+                lane, warp, reg = layout_coords(lay, R, W, K)
+                thr = lane | (warp << 5)
+                for o in e["ops"][ph["op_begin"]:ph["op_end"]]:
+                    m = o["m"].astype(np.float64)
+                    mm = m[0::2] + 1j * m[1::2]
+                    kind, tpos = int(o["kind"]), int(o["tpos"])
+                    ok_t = (base & int(o["cm_glob"])) == int(o["cv_glob"])           # [T]
+                    ok_j = ((thr & int(o["cm_thr"])) == int(o["cv_thr"])) & ((reg & int(o["cm_reg"])) == int(o["cv_reg"]))
+                    if tpos < R:
+                        bit = (reg >> tpos) & 1
+                        if kind in (K_DIAG, K_PHASE):
+                            f = np.where(bit == 1, mm[3], mm[0] if kind == K_DIAG else 1.0)
+                            mask = ok_t[:, None] & ok_j[None, :]
+                            tile = np.where(mask, tile * f[None, :], tile)
+                        else:
+                            sel = np.nonzero((bit == 0) & ok_j)[0]
+                            partner = local_of(lay, R, W, lane[sel], warp[sel], reg[sel] | (1 << tpos))
+                            rows = np.nonzero(ok_t)[0]
+                            a0 = tile[np.ix_(rows, sel)]
+                            a1 = tile[np.ix_(rows, partner)]
+                            if kind == K_SWAP:
+                                n0, n1 = a1, a0
+                            elif kind == K_ANTI:
+                                n0, n1 = mm[1] * a1, mm[2] * a0
+                            else:
+                                n0, n1 = mm[0] * a0 + mm[1] * a1, mm[2] * a0 + mm[3] * a1
+                            tile[np.ix_(rows, sel)] = n0
+                            tile[np.ix_(rows, partner)] = n1
+                    else:
+                        if tpos >= 64:
+                            bv = ((base >> (tpos - 64)) & 1)[:, None] * np.ones((1, 1 << K), dtype=np.int64)
+                        else:
+                            bv = np.broadcast_to(((thr >> (tpos - 8)) & 1)[None, :], (T, 1 << K))
+                        f = np.where(bv == 1, mm[3], mm[0] if kind == K_DIAG else 1.0)
+                        mask = ok_t[:, None] & ok_j[None, :]
+                        tile = np.where(mask, tile * f, tile)
+            state[gidx] = tile
+    return state

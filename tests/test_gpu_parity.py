@@ -13,8 +13,8 @@ from oracle import closed_forms as cf
 from oracle import circuit_lang as cl
 from oracle import cpu
 from simulador_quantico_b200 import workloads as wl
-from tests.helpers import (TOL_F32, TOL_F64, engine_state, fidelity_gap, oracle_state, random_gate_circuit_spec,
-                           random_state)
+from tests.helpers import (TOL_F32, TOL_F64, engine_state, fidelity_gap, min_tiled_qubits, oracle_state,
+                           random_gate_circuit_spec, random_state)
 
 pytestmark = pytest.mark.gpu
 
@@ -45,11 +45,11 @@ def test_reference_truth_tables(sq, name, n, circ, expected, prec):
         assert np.abs(got - want).max() < 1e-6, (name, start)
 
 
-@pytest.mark.parametrize("n", [11, 12, 13, 14])
+@pytest.mark.parametrize("n", [10, 11, 12, 13, 14])
 @pytest.mark.parametrize("warp_bits", [0, 1, 2, 3])
 def test_embedded_truth_tables(sq, n, warp_bits):
     """The same controlled-X truth tables on every placement inside an n-qubit register."""
-    if 10 + warp_bits > n:
+    if min_tiled_qubits("f64", warp_bits) > n:
         pytest.skip("tile larger than state")
     rng = np.random.default_rng(n * 10 + warp_bits)
     for trial in range(6):
@@ -63,13 +63,14 @@ def test_embedded_truth_tables(sq, n, warp_bits):
         assert np.abs(got - want).max() < TOL_F64
 
 
-@pytest.mark.parametrize("n", [3, 9, 10, 11, 12, 13, 15])
+@pytest.mark.parametrize("n", [3, 8, 9, 10, 11, 12, 13, 15])
 @pytest.mark.parametrize("warp_bits", [0, 1, 2, 3])
 @pytest.mark.parametrize("fuse", [1, 0])
 def test_random_gates_f64(sq, n, warp_bits, fuse):
-    if n >= 10 and 10 + warp_bits > n:
+    lo = min_tiled_qubits("f64")
+    if n >= lo and lo + warp_bits > n:
         pytest.skip("tile larger than state")
-    if n < 10 and warp_bits:
+    if n < lo and warp_bits:
         pytest.skip("small-state path has no warp bits")
     spec = random_gate_circuit_spec(n, 6 * n + 12, seed=n * 100 + warp_bits * 10 + fuse)
     init = random_state(n, seed=n)
@@ -88,11 +89,14 @@ def test_random_gates_low_bits(sq, low_bits):
     assert np.abs(got - want).max() < TOL_F64
 
 
-@pytest.mark.parametrize("n", [8, 12, 16])
-@pytest.mark.parametrize("warp_bits", [0, 2, 3])
+@pytest.mark.parametrize("n", [8, 10, 12, 16])
+@pytest.mark.parametrize("warp_bits", [0, 1, 2, 3])
 def test_random_gates_f32(sq, n, warp_bits):
-    if n >= 10 and 10 + warp_bits > n:
+    lo = min_tiled_qubits("f32")
+    if n >= lo and lo + warp_bits > n:
         pytest.skip("tile larger than state")
+    if n < lo and warp_bits:
+        pytest.skip("small-state path has no warp bits")
     spec = random_gate_circuit_spec(n, 5 * n, seed=n + warp_bits)
     init = random_state(n, seed=n + 1)
     got, _ = engine_state(sq, spec, "f32", init=init.astype(np.complex64), warp_bits=warp_bits, renorm_every=0)

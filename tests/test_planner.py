@@ -1,0 +1,80 @@
+"""Planner checks on the CPU: the encoded passes, emulated with numpy
+(tests/plan_emulator.py), reproduce the oracle; plans respect their limits.
+"""
+import numpy as np
+import pytest
+
+import simulador_quantico_b200 as sq
+from simulador_quantico_b200 import workloads as wl
+from tests import plan_emulator as emu
+from tests.helpers import oracle_state, random_gate_circuit_spec, random_state
+
+
+@pytest.mark.parametrize("n", [5, 9, 10, 11, 12, 14])
+@pytest.mark.parametrize("warp_bits", [0, 1, 2, 3])
+@pytest.mark.parametrize("fuse", [0, 1])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_emulated_plan_matches_oracle(n, warp_bits, fuse, prec):
+    R = emu.REG_BITS[prec]
+    if n >= 5 + R and 5 + R + warp_bits > n:
+        pytest.skip("tile larger than state")
+    if n < 5 + R and warp_bits:
+        pytest.skip("small-state path")
+    spec = random_gate_circuit_spec(n, 5 * n, seed=1000 + n * 10 + warp_bits + 100 * fuse)
+    init = random_state(n, seed=n)
+    plan = sq.Plan(spec.build(sq.Circuit()), n, prec, warp_bits=warp_bits, fuse=fuse, renorm_every=0)
+    got = emu.run(plan, prec, init)
+    want = oracle_state(spec, "f64", init=init)
+    assert np.abs(got - want).max() < (1e-12 if prec == "f64" else 1e-5)
+
+
+@pytest.mark.parametrize("low_bits", [0, 2, 5])
+def test_emulated_low_bits(low_bits):
+    n = 13
+    spec = random_gate_circuit_spec(n, 60, seed=low_bits)
+    init = random_state(n, seed=1)
+    plan = sq.Plan(spec.build(sq.Circuit()), n, "f64", low_bits=low_bits, warp_bits=2)
+    assert np.abs(emu.run(plan, "f64", init) - oracle_state(spec, "f64", init=init)).max() < 1e-12
+
+
+@pytest.mark.parametrize("builder", [lambda: wl.random_layered(13, 3, 5), lambda: wl.qft(12, 1234),
+                                     lambda: wl.grover_reference(12, 99, 2), lambda: wl.hadamard_benchmark(14)])
+def test_emulated_workloads(builder):
+    spec = builder()
+    n = spec.qubits
+    plan = sq.Plan(spec.build(sq.Circuit()), n, "f64")
+    init = np.zeros(1 << n, dtype=np.complex128)
+    init[spec.init_index] = 1
+    assert np.abs(emu.run(plan, "f64", init) - oracle_state(spec, "f64")).max() < 1e-12
+
+
+def test_emulated_fp32_encoding():
+    n = 12
+    spec = random_gate_circuit_spec(n, 50, seed=9)
+    init = random_state(n, seed=2)
+    plan = sq.Plan(spec.build(sq.Circuit()), n, "f32", renorm_every=0)
+    got = emu.run(plan, "f32", init)
+    assert np.abs(got - oracle_state(spec, "f64", init=init)).max() < 1e-5
+
+
+def test_plan_pass_counts():
+    """Passes per 30-qubit random layer stay small (planner quality)."""
+    spec = wl.random_layered(30, 4, seed=1)
+    p = sq.Plan(spec.build(sq.Circuit()), 30, "f64")
+    s = p.stats()
+    assert s["ops"] == 4 * 45  # Rz.Ry fused per qubit + 15 CNOTs per layer
+    assert s["passes"] <= 4 * 3
+
+
+def test_grover_plan_fast():
+    """The unrolled 27-qubit Grover (grover.out 27, ~682k PTs) plans in seconds."""
+    import time
+
+    spec = wl.grover_reference(27, 42)
+    c = spec.build(sq.Circuit())
+    assert len(c) == 27 + 106 * 6433
+    t0 = time.time()
+    p = sq.Plan(c, 27, "f64")
+    dt = time.time() - t0
+    assert dt < 20.0
+    assert p.stats()["passes"] < 6 * 6433
