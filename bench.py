@@ -265,7 +265,222 @@ def cpu_baseline_layered(args, kind="reference"):
                       f"to 30 qubits"}
 
 
-WORKLOADS = {"layered": workload_layered}
+
+# ---------------------------------------------------------------------------
+# served stream (continuous batching)
+# ---------------------------------------------------------------------------
+
+SERVED_METRIC = "served circuits/s (FP32 continuous batching, 1-F<1e-6 vs FP64)"
+
+
+def served_requests(seed, count, max_qubits=28):
+    """The serving mix: 60% random layered (12-26 qubits, depth 20), 30% QFT
+    (16-28 qubits) on a random basis input, 10% Grover (14-20 qubits, marked
+    index uniform); all drawn from `seed`."""
+    from simulador_quantico_b200 import workloads as wl
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        u = rng.random()
+        if u < 0.6:
+            n = int(rng.integers(12, 27))
+            spec, mask = wl.random_layered(min(n, max_qubits), 20, seed=seed * 100003 + i), 0
+        elif u < 0.9:
+            n = min(int(rng.integers(16, 29)), max_qubits)
+            spec = wl.qft(n, int(rng.integers(1 << n)))
+            mask = 0
+        else:
+            m = int(rng.integers(14, 21))
+            spec = wl.grover_search(m, int(rng.integers(1 << m)))
+            mask = (1 << m) - 1
+        reqs.append((spec, mask))
+    return reqs
+
+
+def serve_step(sq, srv, reqs, circuits, rate_hz, rng):
+    """Submits `reqs` with Poisson arrivals at rate_hz (0 = all at once) and waits for every result."""
+    t0 = time.perf_counter()
+    gaps = rng.exponential(1.0 / rate_hz, len(reqs)) if rate_hz > 0 else np.zeros(len(reqs))
+    due = t0
+    out = []
+    for (spec, mask), c, gap in zip(reqs, circuits, gaps):
+        due += gap
+        while True:
+            now = time.perf_counter()
+            if now >= due:
+                break
+            out += srv.poll(wait_ms=0)
+            time.sleep(min(0.0005, due - now))
+        srv.submit(c, spec.qubits, spec.init_index, mask)
+    out += srv.drain(len(reqs) - len(out))
+    return out, time.perf_counter() - t0
+
+
+def workload_served(args, dist, sq):
+    count = args.requests or 48
+    steps_reqs = [served_requests(1000 + s, count) for s in range(args.warmup + args.steps)]
+    steps_circuits = [[spec.build(sq.Circuit()) for spec, _ in reqs] for reqs in steps_reqs]
+    srv = sq.Server("f32", budget_bytes=150 << 30, max_inflight=args.inflight)
+    rng = np.random.default_rng(7)
+    for w in range(args.warmup):
+        serve_step(sq, srv, steps_reqs[w], steps_circuits[w], 0, rng)
+    sq.synchronize()
+    dist.barrier()
+    lat, done = [], 0
+    launches0 = sq.kernel_launches()
+    wall = 0.0
+    with ClockSampler(dist.local_rank) as clk:
+        with sq.Timer() as t:
+            for s in range(args.steps):
+                res, dt = serve_step(sq, srv, steps_reqs[args.warmup + s], steps_circuits[args.warmup + s],
+                                     args.rate, rng)
+                wall += dt
+                lat += [r["latency_s"] for r in res]
+                done += len(res)
+                assert all(r["status"] == 0 for r in res)
+            sq.synchronize()
+    launches = sq.kernel_launches() - launches0
+    dist.barrier()
+    ms = dist.max(t.ms)
+    ms_step = ms / args.steps
+    value = dist.sum(done) / (ms * 1e-3)
+    srv.close()
+    lat = np.array(lat)
+    # fidelity of the FP32 served results against FP64 reruns (first timed step)
+    fid = served_fidelity(sq, steps_reqs[args.warmup], steps_circuits[args.warmup]) if not args.skip_fidelity else None
+    # the same requests one by one through the plain FP64 t_GPU drop-in (host states)
+    plain = plain_fp64(sq, steps_reqs[args.warmup], steps_circuits[args.warmup], args.plain_limit) \
+        if not args.skip_e2e else None
+    peak, peak_kind = hbm_peak()
+    line = base_line(args, dist, SERVED_METRIC, value, "circuits/s", ms_step, "f32",
+                     {"workload": f"served-mix-{count}req", "requests_per_step": count, "rate_hz": args.rate,
+                      "max_inflight": args.inflight, "budget_bytes": 150 << 30, "precision": "fp32 amplitudes, "
+                      "fp64 gate matrices, norms and argmax", "mix": "60% layered 12-26q d20, 30% QFT 16-28q, "
+                      "10% Grover 14-20q", "l2": "states up to 2 GiB; no flush (serving keeps states resident)"})
+    line["latency_ms"] = {"p50": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                          "p99": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                          "mean": round(float(lat.mean()) * 1e3, 3)}
+    line["fidelity"] = fid
+    line["plain_fp64"] = plain
+    line["gpu_launches"] = launches
+    line["clocks"] = clk.summary()
+    line["roofline"] = served_roofline(sq, args, peak, peak_kind)
+    line["e2e"] = {"value": round(dist.sum(done) / wall, 4), "unit": "circuits/s",
+                   "h2d_bytes_per_step": None, "d2h_bytes_per_step": 32 * count,
+                   "path": "hgm_server_submit (host circuit, plan + op upload) -> hgm_server_poll (host results)",
+                   "wall_s": round(wall, 3)}
+    if dist.rank == 0 and not args.skip_cpu:
+        line["cpu_baseline"] = cpu_baseline_served(args, steps_reqs[args.warmup])
+    return line
+
+
+def served_fidelity(sq, reqs, circuits):
+    worst_gap, worst_err = 0.0, 0.0
+    for (spec, mask), c in zip(reqs, circuits):
+        a = sq.State(spec.qubits, "f32").set_basis(spec.init_index)
+        a.execute(sq.Plan(c, spec.qubits, "f32"))
+        b = sq.State(spec.qubits, "f64").set_basis(spec.init_index)
+        b.execute(sq.Plan(c, spec.qubits, "f64"))
+        ov = b.inner(a)
+        gap = 1.0 - abs(ov) ** 2 / (a.norm() * b.norm())
+        worst_gap = max(worst_gap, gap)
+        worst_err = max(worst_err, b.max_abs_diff(a))
+        a.free()
+        b.free()
+    return {"max_1_minus_F": worst_gap, "max_abs_amp_err": worst_err, "requests": len(reqs),
+            "ok": bool(worst_gap < 1e-6)}
+
+
+def plain_fp64(sq, reqs, circuits, limit):
+    """The same requests through GpuExecutionWrapper (FP64 drop-in), one by one, host state in and out."""
+    L = sq.load_dropin("f64")
+    L.setDevice(0)
+    t0 = time.perf_counter()
+    k = 0
+    for (spec, mask), c in zip(reqs, circuits):
+        host = np.zeros(1 << spec.qubits, dtype=np.complex128)
+        host[spec.init_index] = 1.0
+        L.GpuExecutionWrapper(host.ctypes.data, c.ref_pts("f64"), spec.qubits, 4, 8, 1, 64, 2, 1)
+        k += 1
+        if limit and time.perf_counter() - t0 > limit:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(k / dt, 4), "unit": "circuits/s", "requests": k, "seconds": round(dt, 3),
+            "path": "GpuExecutionWrapper FP64 (reference C-ABI), host state per request"}
+
+
+def served_roofline(sq, args, peak, peak_kind):
+    """Roofline of the dominant kernel (the FP32 pass kernel) on the mix's largest layered circuit."""
+    from simulador_quantico_b200 import workloads as wl
+
+    n = 26
+    spec = wl.random_layered(n, 20, seed=99)
+    plan = sq.Plan(spec.build(sq.Circuit()), n, "f32")
+    st = sq.State(n, "f32").set_basis(0)
+    st.execute(plan)
+    sq.synchronize()
+    with sq.Timer() as t:
+        st.execute(plan)
+    stats = plan.stats()
+    S = st.nbytes
+    st.free()
+    achieved = stats["passes"] * 2 * S / (t.ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+            "kernel": "pass_kernel<float,%d,%d>" % (stats["reg_bits"], stats["warp_bits"]),
+            "case": f"{n}q FP32 random layered, 20 layers, {stats['passes']} passes",
+            "algorithmic_bytes_per_launch": 2 * S}
+
+
+def cpu_baseline_served(args, reqs, n_cap=20, op_cap=400):
+    """The reference's t_PAR_CPU (FP32, unmodified) on the same request list, each request run on at most
+    n_cap qubits and its first op_cap gates, the time scaled by 2^(n - n_cap) and total/op_cap gates."""
+    from oracle import circuit_lang as cl
+    from oracle import cpu
+
+    threads = os.cpu_count() or 1
+    total_s = 0.0
+    kind = "reference" if cpu.ref_available("f32") else "port"
+    for spec, mask in reqs:
+        full = spec.build(cl.Circuit())
+        t, cm, cv, m = full.as_arrays()
+        n = spec.qubits
+        ns = min(n, n_cap)
+        shift = n - ns
+        keep = [i for i in range(len(t)) if t[i] >= shift and (int(cm[i]) >> shift << shift) == int(cm[i])][:op_cap]
+        ops = (t[keep] - shift, cm[keep] >> shift, cv[keep] >> shift, m[keep])
+        s0 = cpu.basis_state(ns, spec.init_index >> shift, np.complex64)
+        if kind == "reference":
+            r = cpu.RefDGM(ns, "f32")
+            r.set_state(s0)
+            r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
+            # replay the sampled ops through the reference engine as single-gate steps
+            t0 = time.perf_counter()
+            for i in range(len(keep)):
+                name = f"s{i}"
+                r.add_gate(name, ops[3][i])
+                tok = ["ID"] * ns
+                tgt = ns - 1 - int(ops[0][i])
+                cbits = int(ops[1][i])
+                for b in range(ns):
+                    if (cbits >> b) & 1:
+                        tok[ns - 1 - b] = "Control1(1)" if (int(ops[2][i]) >> b) & 1 else "Control1(0)"
+                tok[tgt] = f"Target1({name})" if cbits else name
+                r.set_function(",".join(tok), 1, True)
+                r.execute(1)
+            dt = time.perf_counter() - t0
+            r.close()
+        else:
+            t0 = time.perf_counter()
+            cpu.run_regions(s0, ns, ops, prec="f32", threads=threads)
+            dt = time.perf_counter() - t0
+        total_s += dt * (1 << shift) * (len(t) / max(1, len(keep)))
+    return {"value": round(len(reqs) / total_s, 6), "unit": "circuits/s", "cores": threads, "kind": kind,
+            "sample": f"{len(reqs)} requests of the served mix on t_PAR_CPU FP32; each run on <= {n_cap} qubits "
+                      f"and its first <= {op_cap} gates, time scaled by state size and gate count"}
+
+WORKLOADS = {"layered": workload_layered, "served": workload_served}
 
 
 def base_line(args, dist, metric, value, unit, ms_step, dtype, config):
@@ -278,7 +493,8 @@ def reference_arm(args, dist):
     """The reference's own CPU implementation (t_PAR_CPU), rank 0 only."""
     if dist.rank != 0:
         return None
-    fn = {"layered": cpu_baseline_layered}.get(args.workload)
+    fn = {"layered": cpu_baseline_layered,
+          "served": lambda a: cpu_baseline_served(a, served_requests(1000 + a.warmup, a.requests or 48))}.get(args.workload)
     if fn is None:
         return {"impl": "reference", "unavailable": f"no reference timing for workload {args.workload}"}
     vals = []
@@ -300,14 +516,20 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="layered", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="served", choices=sorted(WORKLOADS))
+    ap.add_argument("--requests", type=int, default=0, help="requests per served step (default 48)")
+    ap.add_argument("--rate", type=float, default=0.0, help="Poisson arrival rate in requests/s (0: all at once)")
+    ap.add_argument("--inflight", type=int, default=16, help="server slots")
+    ap.add_argument("--plain-limit", type=float, default=60.0, help="seconds cap for the plain FP64 comparison")
+    ap.add_argument("--skip-fidelity", action="store_true")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--qubits", type=int, default=0, help="override the workload's qubit count (profiling runs)")
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
     args = ap.parse_args()
-    args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)"}.get(args.workload, args.workload)
+    args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
+                        "served": SERVED_METRIC}.get(args.workload, args.workload)
     dist = Dist()
     try:
         if args.impl == "reference":

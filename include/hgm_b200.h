@@ -167,6 +167,50 @@ int hgm_batch_size(const hgm_batch *b, int *jobs, int64_t *tasks, int64_t *items
 /* A view of one job's state (owned by the batch; hgm_state_free ignores it). */
 hgm_state *hgm_batch_state(hgm_batch *b, int job);
 
+/* ---- serving mode --------------------------------------------------------- */
+/* Continuous batching: circuits are submitted at any time and admitted, in
+ * arrival order, while one of max_inflight slots is free and their state
+ * bytes (16*2^n FP64, 8*2^n FP32) fit budget_bytes; admitted circuits run
+ * concurrently, each on its own stream with a stream-ordered state
+ * allocation; every result reports its FP64 norm, the marginal argmax over
+ * result_mask (if non-zero) and its latency. */
+
+typedef struct hgm_server hgm_server;
+typedef struct hgm_server_opts {
+    int precision;         /* HGM_F64 / HGM_F32 */
+    int64_t budget_bytes;  /* HBM admission budget for resident states */
+    int max_inflight;      /* concurrent requests (streams) */
+    int keep_states;       /* 1: finished states stay on the device until hgm_server_release */
+    int warp_bits;         /* tile size, -1 = default */
+} hgm_server_opts;
+
+typedef struct hgm_result {
+    int64_t id;
+    int status;            /* HGM_OK or an error code */
+    int qubits;
+    double latency_s;      /* submit -> result available */
+    double queue_s;        /* submit -> admitted */
+    double exec_s;         /* admitted -> result available */
+    double norm;           /* sum |a|^2, FP64 */
+    int64_t argmax;        /* marginal argmax over result_mask, -1 if not asked */
+    double pmax;           /* its probability */
+} hgm_result;
+
+void hgm_server_default_opts(hgm_server_opts *o, int precision);
+int hgm_server_create(const hgm_server_opts *opts, hgm_server **out);
+void hgm_server_free(hgm_server *s);
+/* Plans the circuit on the calling thread and queues it. HGM_ERR_BUSY if its
+ * state can never fit the budget. */
+int hgm_server_submit(hgm_server *s, const hgm_circuit *c, int qubits, int64_t init_index, uint64_t result_mask,
+                      int64_t *id);
+/* Moves up to `max` finished results into `out` (waiting up to wait_ms for
+ * the first); *n = how many. */
+int hgm_server_poll(hgm_server *s, hgm_result *out, int max, int *n, int wait_ms);
+int hgm_server_pending(hgm_server *s, int *queued, int *inflight, int64_t *bytes_in_use);
+/* With keep_states: a view of a finished request's state, valid until release. */
+hgm_state *hgm_server_result_state(hgm_server *s, int64_t id);
+int hgm_server_release(hgm_server *s, int64_t id);
+
 /* ---- timing (CUDA events on the library stream) ------------------------- */
 
 /* Records an event pair around everything queued between start and stop. */

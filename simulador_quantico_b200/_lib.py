@@ -24,6 +24,17 @@ class HgmError(RuntimeError):
         self.code = code
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("budget_bytes", C.c_int64), ("max_inflight", C.c_int),
+                ("keep_states", C.c_int), ("warp_bits", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int), ("qubits", C.c_int), ("latency_s", C.c_double),
+                ("queue_s", C.c_double), ("exec_s", C.c_double), ("norm", C.c_double), ("argmax", C.c_int64),
+                ("pmax", C.c_double)]
+
+
 class PlanOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("warp_bits", C.c_int), ("low_bits", C.c_int), ("fuse", C.c_int),
                 ("window", C.c_int), ("renorm_every", C.c_int)]
@@ -80,6 +91,14 @@ def _load():
         "hgm_batch_check": ([vp], i),
         "hgm_batch_size": ([vp, P(i), P(i64), P(i64), P(i64)], i),
         "hgm_batch_state": ([vp, i], vp),
+        "hgm_server_default_opts": ([P(ServerOpts), i], None),
+        "hgm_server_create": ([P(ServerOpts), P(vp)], i),
+        "hgm_server_free": ([vp], None),
+        "hgm_server_submit": ([vp, vp, i, i64, C.c_uint64, P(i64)], i),
+        "hgm_server_poll": ([vp, P(Result), i, P(i), i], i),
+        "hgm_server_pending": ([vp, P(i), P(i), P(i64)], i),
+        "hgm_server_result_state": ([vp, i64], vp),
+        "hgm_server_release": ([vp, i64], i),
         "hgm_timer_start": ([], i),
         "hgm_timer_stop": ([P(d)], i),
     }

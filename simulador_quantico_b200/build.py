@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}", "-ccbin", "g++"]
 
-ENGINE_SRCS = ["circuit.cpp", "planner.cpp", "engine.cpp", "kernels.cu", "batch.cu"]
+ENGINE_SRCS = ["circuit.cpp", "planner.cpp", "engine.cpp", "kernels.cu", "batch.cu", "server.cpp"]
 # Extra nvcc flags (e.g. -DHGM_MAXREG_F32=128) and an alternative output
 # folder, for building tuning variants side by side.
 EXTRA_FLAGS = os.environ.get("HGM_NVCC_EXTRA", "").split()
@@ -67,7 +67,8 @@ def build(verbose: bool = False, ptxas_verbose: bool = False, lib_dir: Path | No
         objs.append(o)
     engine = LIB / "libhgm_b200.so"
     if _stale(engine, objs):
-        _run([nvcc, *ARCH, "-shared", "-o", engine, *objs, "-Xlinker", "-soname=libhgm_b200.so"], verbose)
+        _run([nvcc, *ARCH, "-shared", "-o", engine, *objs, "-Xlinker", "-soname=libhgm_b200.so", "-lpthread"],
+             verbose)
     for prec, define in (("f32", []), ("f64", ["-DHGM_DROPIN_F64"])):
         so = LIB / f"libhgm_dropin_{prec}.so"
         src = CSRC / "dropin.cpp"

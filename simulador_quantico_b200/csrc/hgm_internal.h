@@ -59,6 +59,9 @@ enum DevKind : int32_t {
     K_PHASE = 3,   // diag(1, m11)
     K_ANTI = 4,    // [[0, m01], [m10, 0]]
     K_SWAP = 5,    // [[0, 1], [1, 0]]
+    K_LAYER = 6,   // one uncontrolled dense gate on every register bit; the
+                   // R matrices follow in the next R records (bit 0 first)
+    K_LAYER_REAL = 7,  // the same with real matrices
 };
 
 // Target location codes inside a phase: 0..R-1 register bit, 8+q thread bit q
@@ -71,6 +74,7 @@ struct alignas(16) DevOp {
     int32_t kind, tpos;
     uint32_t cm_reg, cv_reg;   // controls on register bits
     uint32_t cm_thr, cv_thr;   // controls on thread bits (lane | warp << 5)
+    uint32_t pad0, pad1;
     uint64_t cm_glob, cv_glob; // controls on non-tile index bits
     Real m[8];
 };
@@ -155,6 +159,14 @@ int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *s
 int inner(State *a, State *b, double *re, double *im, void *stream);
 int max_abs_diff(State *a, State *b, double *out, void *stream);
 int scale_state(State *s, double scale, void *stream);
+
+// Asynchronous FP64 reductions into caller-owned device scratch (used by
+// concurrent clients such as the server's slots): partials holds
+// 2*REDUCE_SCRATCH_BLOCKS doubles, ibest REDUCE_SCRATCH_BLOCKS indices;
+// norm -> out[0]; marginal argmax probability -> out[0], index -> out[1].
+constexpr int REDUCE_SCRATCH_BLOCKS = 1184;
+int launch_norm_async(State *s, double *partials, double *out, void *stream);
+int launch_argmax_async(State *s, uint64_t mask, double *pbest, long long *ibest, double *out, void *stream);
 
 void *default_stream();
 void count_launch(int n = 1);

@@ -23,7 +23,7 @@ namespace hgm {
 // ---------------------------------------------------------------------------
 
 namespace {
-constexpr int RED_BLOCKS = 1184;   // 8 x 148 SMs
+constexpr int RED_BLOCKS = REDUCE_SCRATCH_BLOCKS;   // 8 x 148 SMs
 constexpr int RED_THREADS = 256;
 
 struct Ctx {
@@ -416,6 +416,19 @@ static int run_reduce(const void *a, const void *b, int qubits, int bit, double 
     return HGM_OK;
 }
 
+int launch_norm_async(State *s, double *partials, double *out, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long N = 1ll << s->qubits;
+    const unsigned g = grid_for(N);
+    if (s->precision == HGM_F64)
+        reduce_kernel<double, double, RED_NORM><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, nullptr, N, 0, partials);
+    else
+        reduce_kernel<float, float, RED_NORM><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, nullptr, N, 0, partials);
+    reduce_final<RED_NORM><<<1, 32, 0, st>>>(partials, (int)g, out);
+    count_launch(2);
+    return check("norm reduction launch");
+}
+
 int reduce_norm(State *s, double *out, void *stream) {
     cudaStream_t st = pick(stream);
     if (!st) return HGM_ERR_CUDA;
@@ -520,6 +533,24 @@ __global__ void marginal_final(const double *pbest, const long long *ibest, int 
         out[0] = b;
         out[1] = (double)bi;
     }
+}
+
+int launch_argmax_async(State *s, uint64_t mask, double *pbest, long long *ibest, double *out, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = s->qubits;
+    if (n < 64 && (mask >> n)) return fail(HGM_ERR_INVALID, "mask beyond state bits");
+    const int m = __builtin_popcountll(mask);
+    const long long M = 1ll << m;
+    unsigned g = (unsigned)((M + RED_THREADS - 1) / RED_THREADS);
+    if (g > RED_BLOCKS) g = RED_BLOCKS;
+    if (g < 1) g = 1;
+    if (s->precision == HGM_F64)
+        marginal_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, m, pbest, ibest);
+    else
+        marginal_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, m, pbest, ibest);
+    marginal_final<<<1, 32, 0, st>>>(pbest, ibest, (int)g, out);
+    count_launch(2);
+    return check("argmax launch");
 }
 
 int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *stream) {

@@ -275,36 +275,87 @@ __device__ __forceinline__ void reg_kind(int kind, A2 (&a)[1 << R], const Real (
     else reg_kind_c<Real, A2, R, T, true>(kind, a, m, cm, cv);
 }
 
+template <typename Real>
+__device__ __forceinline__ void load_matrix(const Real *__restrict__ src, Real (&m)[8]);
+template <>
+__device__ __forceinline__ void load_matrix<double>(const double *__restrict__ src, double (&m)[8]) {
+    const double2 *p = reinterpret_cast<const double2 *>(src);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double2 v = __ldg(p + k);
+        m[2 * k] = v.x;
+        m[2 * k + 1] = v.y;
+    }
+}
+template <>
+__device__ __forceinline__ void load_matrix<float>(const float *__restrict__ src, float (&m)[8]) {
+    const float4 *p = reinterpret_cast<const float4 *>(src);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float4 v = __ldg(p + k);
+        m[4 * k] = v.x;
+        m[4 * k + 1] = v.y;
+        m[4 * k + 2] = v.z;
+        m[4 * k + 3] = v.w;
+    }
+}
+
+// A full layer: one uncontrolled dense gate on each register bit, applied
+// bit 0 first, in one straight-line block (no per-gate dispatch).
+template <typename Real, typename A2, int R, int T, bool REAL>
+struct LayerStep {
+    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats) {
+        Real m[8];
+        load_matrix<Real>(mats[T].m, m);
+        if (REAL) reg_real<Real, A2, R, T, false>(a, m, 0u, 0u);
+        else reg_dense<Real, A2, R, T, false>(a, m, 0u, 0u);
+        LayerStep<Real, A2, R, T + 1, REAL>::run(a, mats);
+    }
+};
+template <typename Real, typename A2, int R, bool REAL>
+struct LayerStep<Real, A2, R, R, REAL> {
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__) {}
+};
+
+// Applies record `op` (and, for a layer, its matrix records); returns the
+// number of records consumed.
 template <typename Real, typename A2, int R>
-__device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, uint64_t base,
-                                         uint32_t thr) {
-    const uint64_t cmg = __ldg(reinterpret_cast<const unsigned long long *>(&op->cm_glob));
-    const uint64_t cvg = __ldg(reinterpret_cast<const unsigned long long *>(&op->cv_glob));
-    if ((base & cmg) != cvg) return;
+__device__ __forceinline__ int apply_op(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, uint64_t base,
+                                        uint32_t thr) {
     const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));  // kind, tpos, cm_reg, cv_reg
-    const uint2 th = __ldg(reinterpret_cast<const uint2 *>(&op->cm_thr));
-    if ((thr & th.x) != th.y) return;
     const int kind = (int)hdr.x, tpos = (int)hdr.y;
+    if (kind == K_LAYER) {
+        LayerStep<Real, A2, R, 0, false>::run(a, op + 1);
+        return 1 + R;
+    }
+    if (kind == K_LAYER_REAL) {
+        LayerStep<Real, A2, R, 0, true>::run(a, op + 1);
+        return 1 + R;
+    }
+    const uint4 th = __ldg(reinterpret_cast<const uint4 *>(op) + 1);                 // cm_thr, cv_thr
+    const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(op) + 2);       // cm_glob, cv_glob
+    if ((base & gl.x) != gl.y) return 1;
+    if ((thr & th.x) != th.y) return 1;
     const uint32_t cm = hdr.z, cv = hdr.w;
     Real m[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) m[k] = __ldg(&op->m[k]);
+    load_matrix<Real>(op->m, m);
     if (tpos < R) {
         switch (tpos) {
-            case 0: reg_kind<Real, A2, R, 0>(kind, a, m, cm, cv); return;
-            case 1: reg_kind<Real, A2, R, 1>(kind, a, m, cm, cv); return;
-            case 2: reg_kind<Real, A2, R, 2>(kind, a, m, cm, cv); return;
-            case 3: reg_kind<Real, A2, R, 3>(kind, a, m, cm, cv); return;
-            default: reg_kind<Real, A2, R, (R > 4 ? 4 : 3)>(kind, a, m, cm, cv); return;
+            case 0: reg_kind<Real, A2, R, 0>(kind, a, m, cm, cv); return 1;
+            case 1: reg_kind<Real, A2, R, 1>(kind, a, m, cm, cv); return 1;
+            case 2: reg_kind<Real, A2, R, 2>(kind, a, m, cm, cv); return 1;
+            case 3: reg_kind<Real, A2, R, 3>(kind, a, m, cm, cv); return 1;
+            default: reg_kind<Real, A2, R, (R > 4 ? 4 : 3)>(kind, a, m, cm, cv); return 1;
         }
     }
     // diagonal gate on a thread bit or a non-tile index bit
     const int bv = tpos >= TPOS_GLOBAL ? (int)((base >> (tpos - TPOS_GLOBAL)) & 1)
                                        : (int)((thr >> (tpos - TPOS_THREAD)) & 1);
-    if (kind == K_PHASE && !bv) return;
+    if (kind == K_PHASE && !bv) return 1;
     const Real fr = bv ? m[6] : m[0], fi = bv ? m[7] : m[1];
     if (cm == 0) reg_scale<Real, A2, R, false>(a, fr, fi, cm, cv);
     else reg_scale<Real, A2, R, true>(a, fr, fi, cm, cv);
+    return 1;
 }
 
 // ---- layout transposes through shared memory --------------------------------
@@ -418,7 +469,7 @@ __device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ stat
             prev_cross = ph.xwarp != 0;
             cur = ph.layout;
         }
-        for (int i = ph.op_begin; i < ph.op_end; i++) apply_op<Real, A2, R>(a, ops + i, base, thr);
+        for (int i = ph.op_begin; i < ph.op_end;) i += apply_op<Real, A2, R>(a, ops + i, base, thr);
     }
     if (cur != pa.store_layout) {
         const bool cross = (cur == LAYOUT_A) != (pa.store_layout == LAYOUT_A);

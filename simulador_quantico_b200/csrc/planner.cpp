@@ -167,6 +167,56 @@ DevOp<Real> encode(const SOp &o, int layout, int R, int W, const int loc_of[64],
     return d;
 }
 
+// Emits a phase's gates.  Uncontrolled dense gates that cover every
+// register bit of the layout, and that can all move to the front of what is
+// left (each commutes with every other gate before it), become one K_LAYER
+// record followed by their R matrices (register bit 0 first); the rest are
+// emitted one record each, in order.
+template <typename Real>
+void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, int R, int W, const int loc_of[64],
+                uint64_t tmask, std::vector<DevOp<Real>> &out) {
+    for (;;) {
+        int slot[8];
+        for (int k = 0; k < 8; k++) slot[k] = -1;
+        int found = 0;
+        bool all_real = true;
+        uint64_t bn = 0, bd = 0;
+        for (int idx : rest) {
+            const SOp &op = ops[idx];
+            bool cand = false;
+            if (op.mc == MC_DENSE && op.cmask == 0 && !conflicts(op, bn, bd)) {
+                Role rl = role(layout, R, W, loc_of[op.target]);
+                if (rl.kind == ROLE_REG && slot[rl.idx] < 0) {
+                    slot[rl.idx] = idx;
+                    found++;
+                    cand = true;
+                    for (int k = 0; k < 4; k++) all_real = all_real && op.m[k].imag() == 0;
+                }
+            }
+            if (!cand) {
+                bn |= op.nd();
+                bd |= op.dg();
+            }
+            if (found == R) break;
+        }
+        if (found < R) break;
+        DevOp<Real> head;
+        memset(&head, 0, sizeof head);
+        head.kind = all_real ? K_LAYER_REAL : K_LAYER;
+        head.tpos = R;
+        out.push_back(head);
+        std::vector<int> keep;
+        for (int k = 0; k < R; k++) out.push_back(encode<Real>(ops[slot[k]], layout, R, W, loc_of, tmask));
+        for (int idx : rest) {
+            bool member = false;
+            for (int k = 0; k < R; k++) member = member || slot[k] == idx;
+            if (!member) keep.push_back(idx);
+        }
+        rest.swap(keep);
+    }
+    for (int idx : rest) out.push_back(encode<Real>(ops[idx], layout, R, W, loc_of, tmask));
+}
+
 template <typename Real>
 SmallOp<Real> encode_small(const SOp &o) {
     SmallOp<Real> s;
@@ -337,7 +387,7 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
             DevPhase ph;
             ph.layout = best;
             ph.op_begin = (int)dev_ops.size();
-            for (int idx : taken) dev_ops.push_back(encode<Real>(ops[idx], best, R, W, loc_of, tmask));
+            emit_phase<Real>(ops, taken, best, R, W, loc_of, tmask, dev_ops);
             ph.op_end = (int)dev_ops.size();
             int prev = cur < 0 ? (best == LAYOUT_A ? LAYOUT_A : LAYOUT_C) : cur;
             ph.xwarp = (prev != best) && (prev == LAYOUT_A || best == LAYOUT_A) ? 1 : 0;

@@ -1,0 +1,347 @@
+// Serving mode: continuous batching of circuits on one GPU.
+//
+// Clients submit circuits at any time (hgm_server_submit plans them on the
+// calling thread).  One worker thread
+//   * admits queued requests in arrival order while a slot is free and the
+//     request's state bytes (16*2^n FP64, 8*2^n FP32) fit the HBM budget
+//     (a request larger than the whole budget is refused);
+//   * gives each admitted request a slot -- a CUDA stream with its own
+//     reduction scratch -- allocates the state stream-ordered
+//     (cudaMallocAsync from the device's memory pool, so no allocation
+//     synchronises the device), initialises it, queues the plan's passes, an
+//     FP64 norm and (if asked) the marginal argmax, copies those few numbers
+//     to pinned host memory and records an event;
+//   * polls the slots' events; a finished request records its completion
+//     time, frees (or keeps) its state and frees the slot for the next one.
+// Requests on different slots run concurrently on the device; new requests
+// are admitted while earlier ones are still executing.  A request's result
+// does not depend on what else runs: it uses its own plan, state and scratch
+// and fixed-order reductions.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "hgm_internal.h"
+
+namespace hgm {
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+    int64_t id = 0;
+    int n = 0;
+    int64_t init_index = 0;
+    uint64_t result_mask = 0;
+    std::unique_ptr<Plan> plan;
+    int64_t bytes = 0;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    State state;  // device state (pool memory)
+    int status = HGM_OK;
+    double norm = 0, pmax = 0;
+    int64_t argmax = -1;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    double *partials = nullptr;
+    long long *ibest = nullptr;
+    double *dres = nullptr;   // 4 doubles
+    double *hres = nullptr;   // pinned, 4 doubles
+    Request *req = nullptr;
+};
+
+}  // namespace
+
+struct Server {
+    hgm_server_opts opts;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Request *> queue;
+    std::vector<Slot> slots;
+    std::map<int64_t, Request *> kept;      // finished requests whose states are kept
+    std::deque<hgm_result> results;
+    std::condition_variable results_cv;
+    int64_t bytes_in_use = 0;
+    int64_t next_id = 1;
+    std::atomic<bool> stop{false};
+    std::thread worker;
+    int inflight = 0;
+    int error = HGM_OK;
+
+    ~Server() {
+        stop = true;
+        cv.notify_all();
+        if (worker.joinable()) worker.join();
+        for (Slot &s : slots) {
+            if (s.stream) cudaStreamSynchronize(s.stream);
+            if (s.req) {
+                if (s.req->state.d) cudaFreeAsync(s.req->state.d, s.stream);
+                delete s.req;
+            }
+            if (s.partials) cudaFree(s.partials);
+            if (s.ibest) cudaFree(s.ibest);
+            if (s.dres) cudaFree(s.dres);
+            if (s.hres) cudaFreeHost(s.hres);
+            if (s.done) cudaEventDestroy(s.done);
+            if (s.stream) cudaStreamDestroy(s.stream);
+        }
+        for (Request *r : queue) delete r;
+        for (auto &kv : kept) {
+            if (kv.second->state.d) cudaFreeAsync(kv.second->state.d, (cudaStream_t)default_stream());
+            delete kv.second;
+        }
+    }
+
+    void finish(Slot &s) {
+        Request *r = s.req;
+        r->t_done = now_s();
+        r->norm = s.hres[0];
+        if (r->result_mask) {
+            r->pmax = s.hres[2];
+            r->argmax = (int64_t)s.hres[3];
+        }
+        hgm_result res;
+        res.id = r->id;
+        res.status = r->status;
+        res.qubits = r->n;
+        res.latency_s = r->t_done - r->t_submit;
+        res.queue_s = r->t_admit - r->t_submit;
+        res.exec_s = r->t_done - r->t_admit;
+        res.norm = r->norm;
+        res.argmax = r->argmax;
+        res.pmax = r->pmax;
+        if (opts.keep_states) {
+            std::lock_guard<std::mutex> lk(mu);
+            kept[r->id] = r;
+        } else {
+            cudaFreeAsync(r->state.d, s.stream);
+            r->state.d = nullptr;
+            std::lock_guard<std::mutex> lk(mu);
+            bytes_in_use -= r->bytes;
+            delete r;
+        }
+        s.req = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            results.push_back(res);
+            inflight--;
+        }
+        results_cv.notify_all();
+    }
+
+    int start(Slot &s, Request *r) {
+        r->t_admit = now_s();
+        s.req = r;
+        cudaError_t e = cudaMallocAsync(&r->state.d, (size_t)r->bytes, s.stream);
+        if (e != cudaSuccess) return fail(HGM_ERR_NOMEM, "request state: %s", cudaGetErrorString(e));
+        r->state.qubits = r->n;
+        r->state.precision = opts.precision;
+        int rc = launch_set_basis(&r->state, r->init_index, s.stream);
+        if (!rc) rc = launch_plan(&r->state, r->plan.get(), 1, s.stream);
+        if (!rc) rc = launch_norm_async(&r->state, s.partials, s.dres, s.stream);
+        if (!rc && r->result_mask) rc = launch_argmax_async(&r->state, r->result_mask, s.partials, s.ibest, s.dres + 2, s.stream);
+        if (rc) return rc;
+        cudaMemcpyAsync(s.hres, s.dres, 4 * sizeof(double), cudaMemcpyDeviceToHost, s.stream);
+        e = cudaEventRecord(s.done, s.stream);
+        return e == cudaSuccess ? HGM_OK : fail(HGM_ERR_CUDA, "event record: %s", cudaGetErrorString(e));
+    }
+
+    int device = 0;
+
+    void loop() {
+        cudaSetDevice(device);
+        while (!stop) {
+            bool progress = false;
+            // completions
+            for (Slot &s : slots) {
+                if (!s.req) continue;
+                cudaError_t q = cudaEventQuery(s.done);
+                if (q == cudaSuccess) {
+                    finish(s);
+                    progress = true;
+                } else if (q != cudaErrorNotReady) {
+                    s.req->status = HGM_ERR_CUDA;
+                    error = fail(HGM_ERR_CUDA, "request execution: %s", cudaGetErrorString(q));
+                    finish(s);
+                    progress = true;
+                }
+            }
+            // admissions, in arrival order
+            for (Slot &s : slots) {
+                if (s.req) continue;
+                Request *r = nullptr;
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    if (queue.empty()) break;
+                    if (bytes_in_use + queue.front()->bytes > opts.budget_bytes) break;
+                    r = queue.front();
+                    queue.pop_front();
+                    bytes_in_use += r->bytes;
+                    inflight++;
+                }
+                int rc = start(s, r);
+                if (rc) {
+                    r->status = rc;
+                    cudaStreamSynchronize(s.stream);
+                    finish(s);
+                }
+                progress = true;
+            }
+            if (!progress) {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait_for(lk, std::chrono::microseconds(inflight ? 20 : 500));
+            }
+        }
+    }
+};
+
+}  // namespace hgm
+
+using namespace hgm;
+
+extern "C" {
+
+void hgm_server_default_opts(hgm_server_opts *o, int precision) {
+    o->precision = precision;
+    o->budget_bytes = (int64_t)150 << 30;
+    o->max_inflight = 16;
+    o->keep_states = 0;
+    o->warp_bits = -1;
+}
+
+int hgm_server_create(const hgm_server_opts *opts, hgm_server **out) {
+    if (!opts || !out) return fail(HGM_ERR_INVALID, "null argument");
+    if (opts->max_inflight < 1 || opts->max_inflight > 256) return fail(HGM_ERR_INVALID, "max_inflight outside 1..256");
+    if (!default_stream()) return HGM_ERR_CUDA;
+    std::unique_ptr<Server> s(new Server());
+    s->opts = *opts;
+    // keep freed request memory in the pool up to the budget (no trimming on every free)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = (uint64_t)opts->budget_bytes;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    s->slots.resize(opts->max_inflight);
+    for (Slot &sl : s->slots) {
+        cudaError_t e;
+        if ((e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaMalloc(&sl.partials, 2 * REDUCE_SCRATCH_BLOCKS * sizeof(double))) != cudaSuccess ||
+            (e = cudaMalloc(&sl.ibest, REDUCE_SCRATCH_BLOCKS * sizeof(long long))) != cudaSuccess ||
+            (e = cudaMalloc(&sl.dres, 4 * sizeof(double))) != cudaSuccess ||
+            (e = cudaMallocHost(&sl.hres, 4 * sizeof(double))) != cudaSuccess)
+            return fail(HGM_ERR_CUDA, "server slot: %s", cudaGetErrorString(e));
+    }
+    cudaGetDevice(&s->device);
+    Server *raw = s.get();
+    s->worker = std::thread([raw] { raw->loop(); });
+    *out = reinterpret_cast<hgm_server *>(s.release());
+    return HGM_OK;
+}
+
+void hgm_server_free(hgm_server *s) { delete reinterpret_cast<Server *>(s); }
+
+int hgm_server_submit(hgm_server *ss, const hgm_circuit *c, int qubits, int64_t init_index, uint64_t result_mask,
+                      int64_t *id) {
+    Server *s = reinterpret_cast<Server *>(ss);
+    if (!s || !c) return fail(HGM_ERR_INVALID, "null argument");
+    if (init_index < 0 || init_index >= (int64_t(1) << qubits)) return fail(HGM_ERR_INVALID, "initial index outside state");
+    std::unique_ptr<Request> r(new Request());
+    r->t_submit = now_s();
+    r->n = qubits;
+    r->init_index = init_index;
+    r->result_mask = result_mask;
+    r->bytes = (int64_t(1) << qubits) * (s->opts.precision == HGM_F64 ? 16 : 8);
+    if (r->bytes > s->opts.budget_bytes)
+        return fail(HGM_ERR_BUSY, "state of %lld bytes exceeds the %lld-byte budget", (long long)r->bytes,
+                    (long long)s->opts.budget_bytes);
+    hgm_plan_opts o;
+    hgm_plan_default_opts(&o, s->opts.precision);
+    o.warp_bits = s->opts.warp_bits;
+    r->plan.reset(new Plan());
+    int rc = build_plan(reinterpret_cast<const Circuit *>(c)->ops, qubits, o, r->plan.get());
+    if (!rc) rc = upload_plan(r->plan.get());
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        if (id) *id = r->id;
+        s->queue.push_back(r.release());
+    }
+    s->cv.notify_all();
+    return HGM_OK;
+}
+
+int hgm_server_poll(hgm_server *ss, hgm_result *out, int max, int *n, int wait_ms) {
+    Server *s = reinterpret_cast<Server *>(ss);
+    if (!s || !out || !n) return fail(HGM_ERR_INVALID, "null argument");
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->results.empty() && wait_ms > 0)
+        s->results_cv.wait_for(lk, std::chrono::milliseconds(wait_ms), [s] { return !s->results.empty(); });
+    int k = 0;
+    while (k < max && !s->results.empty()) {
+        out[k++] = s->results.front();
+        s->results.pop_front();
+    }
+    *n = k;
+    return s->error;
+}
+
+int hgm_server_pending(hgm_server *ss, int *queued, int *inflight, int64_t *bytes_in_use) {
+    Server *s = reinterpret_cast<Server *>(ss);
+    if (!s) return fail(HGM_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (queued) *queued = (int)s->queue.size();
+    if (inflight) *inflight = s->inflight;
+    if (bytes_in_use) *bytes_in_use = s->bytes_in_use;
+    return HGM_OK;
+}
+
+hgm_state *hgm_server_result_state(hgm_server *ss, int64_t id) {
+    Server *s = reinterpret_cast<Server *>(ss);
+    if (!s) return nullptr;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->kept.find(id);
+    if (it == s->kept.end()) {
+        fail(HGM_ERR_INVALID, "request %lld has no kept state", (long long)id);
+        return nullptr;
+    }
+    it->second->state.owned = false;
+    return reinterpret_cast<hgm_state *>(&it->second->state);
+}
+
+int hgm_server_release(hgm_server *ss, int64_t id) {
+    Server *s = reinterpret_cast<Server *>(ss);
+    if (!s) return fail(HGM_ERR_INVALID, "null server");
+    Request *r = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->kept.find(id);
+        if (it == s->kept.end()) return fail(HGM_ERR_INVALID, "request %lld has no kept state", (long long)id);
+        r = it->second;
+        s->kept.erase(it);
+        s->bytes_in_use -= r->bytes;
+    }
+    cudaFreeAsync(r->state.d, (cudaStream_t)default_stream());
+    delete r;
+    s->cv.notify_all();
+    return HGM_OK;
+}
+
+}  // extern "C"

@@ -252,6 +252,66 @@ class Batch:
         return State.view(h, self.qubits[job], self.precision, owner=self)
 
 
+class Server:
+    """Continuous-batching server (include/hgm_b200.h, serving mode)."""
+
+    def __init__(self, precision="f32", budget_bytes=150 << 30, max_inflight=16, keep_states=False, warp_bits=-1):
+        init()
+        o = _lib.ServerOpts()
+        lib.hgm_server_default_opts(C.byref(o), PREC[precision])
+        o.budget_bytes, o.max_inflight, o.keep_states, o.warp_bits = budget_bytes, max_inflight, int(keep_states), warp_bits
+        self.precision = PREC[precision]
+        self.h = C.c_void_p()
+        self.qubits = {}
+        check(lib.hgm_server_create(C.byref(o), C.byref(self.h)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.hgm_server_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, circuit: Circuit, qubits: int, init_index: int = 0, result_mask: int = 0) -> int:
+        rid = C.c_int64()
+        check(lib.hgm_server_submit(self.h, circuit.h, qubits, init_index, result_mask, C.byref(rid)))
+        self.qubits[rid.value] = qubits
+        return rid.value
+
+    def poll(self, max_results=256, wait_ms=0):
+        buf = (_lib.Result * max_results)()
+        n = C.c_int()
+        check(lib.hgm_server_poll(self.h, buf, max_results, C.byref(n), wait_ms))
+        return [dict(id=r.id, status=r.status, qubits=r.qubits, latency_s=r.latency_s, queue_s=r.queue_s,
+                     exec_s=r.exec_s, norm=r.norm, argmax=r.argmax, pmax=r.pmax) for r in buf[:n.value]]
+
+    def pending(self):
+        q, f, b = C.c_int(), C.c_int(), C.c_int64()
+        check(lib.hgm_server_pending(self.h, C.byref(q), C.byref(f), C.byref(b)))
+        return dict(queued=q.value, inflight=f.value, bytes_in_use=b.value)
+
+    def drain(self, expected, timeout_s=600.0):
+        """Collects results until `expected` have arrived."""
+        import time as _t
+
+        out, t0 = [], _t.time()
+        while len(out) < expected:
+            out += self.poll(wait_ms=50)
+            if _t.time() - t0 > timeout_s:
+                raise TimeoutError(f"{len(out)}/{expected} results after {timeout_s} s")
+        return out
+
+    def result_state(self, rid: int) -> State:
+        h = lib.hgm_server_result_state(self.h, rid)
+        if not h:
+            raise _lib.HgmError(1, _lib.last_error())
+        return State.view(h, self.qubits[rid], self.precision, owner=self)
+
+    def release(self, rid: int):
+        check(lib.hgm_server_release(self.h, rid))
+
+
 def synchronize():
     check(lib.hgm_synchronize())
 

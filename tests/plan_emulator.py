@@ -24,7 +24,8 @@ PHASE_DT = np.dtype([("layout", "<i4"), ("op_begin", "<i4"), ("op_end", "<i4"), 
 
 def op_dtype(real):
     fields = [("kind", "<i4"), ("tpos", "<i4"), ("cm_reg", "<u4"), ("cv_reg", "<u4"), ("cm_thr", "<u4"),
-              ("cv_thr", "<u4"), ("cm_glob", "<u8"), ("cv_glob", "<u8"), ("m", real, 8)]
+              ("cv_thr", "<u4"), ("pad0", "<u4"), ("pad1", "<u4"), ("cm_glob", "<u8"), ("cv_glob", "<u8"),
+              ("m", real, 8)]
     dt = np.dtype(fields)
     size = (dt.itemsize + 15) // 16 * 16
     return np.dtype({"names": dt.names, "formats": [dt.fields[n][0] for n in dt.names],
@@ -34,7 +35,7 @@ def op_dtype(real):
 SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f8", 8)]),
             "<f4": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f4", 8)])}
 
-K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP = range(6)
+K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL = range(8)
 LAYOUT_C, LAYOUT_B, LAYOUT_A, LAYOUT_E = 0, 1, 2, 3
 REG_BITS = {"f64": 4, "f32": 5}
 
@@ -94,6 +95,24 @@ def apply_small(state, ops, n):
     return state
 
 
+def apply_reg_pair(tile, lay, R, W, lane, warp, reg, tpos, ok_t, ok_j, kind, mm):
+    bit = (reg >> tpos) & 1
+    sel = np.nonzero((bit == 0) & ok_j)[0]
+    partner = local_of(lay, R, W, lane[sel], warp[sel], reg[sel] | (1 << tpos))
+    rows = np.nonzero(ok_t)[0]
+    a0 = tile[np.ix_(rows, sel)]
+    a1 = tile[np.ix_(rows, partner)]
+    if kind == K_SWAP:
+        n0, n1 = a1, a0
+    elif kind == K_ANTI:
+        n0, n1 = mm[1] * a1, mm[2] * a0
+    else:
+        n0, n1 = mm[0] * a0 + mm[1] * a1, mm[2] * a0 + mm[3] * a1
+    tile[np.ix_(rows, sel)] = n0
+    tile[np.ix_(rows, partner)] = n1
+    return tile
+
+
 def run(plan, precision, state, iterations=1):
     e = export(plan, precision)
     n = plan.qubits
@@ -125,7 +144,20 @@ def run(plan, precision, state, iterations=1):
                 lay = int(ph["layout"])
                 lane, warp, reg = layout_coords(lay, R, W, K)
                 thr = lane | (warp << 5)
-                for o in e["ops"][ph["op_begin"]:ph["op_end"]]:
+                recs = e["ops"][ph["op_begin"]:ph["op_end"]]
+                i = 0
+                while i < len(recs):
+                    o = recs[i]
+                    if int(o["kind"]) in (K_LAYER, K_LAYER_REAL):
+                        # R uncontrolled dense gates, register bit 0 first
+                        for t in range(R):
+                            mm = recs[i + 1 + t]["m"].astype(np.float64)
+                            mm = mm[0::2] + 1j * mm[1::2]
+                            tile = apply_reg_pair(tile, lay, R, W, lane, warp, reg, t, np.ones(T, bool),
+                                                  np.ones(1 << K, bool), K_DENSE, mm)
+                        i += 1 + R
+                        continue
+                    i += 1
                     m = o["m"].astype(np.float64)
                     mm = m[0::2] + 1j * m[1::2]
                     kind, tpos = int(o["kind"]), int(o["tpos"])
@@ -138,19 +170,7 @@ def run(plan, precision, state, iterations=1):
                             mask = ok_t[:, None] & ok_j[None, :]
                             tile = np.where(mask, tile * f[None, :], tile)
                         else:
-                            sel = np.nonzero((bit == 0) & ok_j)[0]
-                            partner = local_of(lay, R, W, lane[sel], warp[sel], reg[sel] | (1 << tpos))
-                            rows = np.nonzero(ok_t)[0]
-                            a0 = tile[np.ix_(rows, sel)]
-                            a1 = tile[np.ix_(rows, partner)]
-                            if kind == K_SWAP:
-                                n0, n1 = a1, a0
-                            elif kind == K_ANTI:
-                                n0, n1 = mm[1] * a1, mm[2] * a0
-                            else:
-                                n0, n1 = mm[0] * a0 + mm[1] * a1, mm[2] * a0 + mm[3] * a1
-                            tile[np.ix_(rows, sel)] = n0
-                            tile[np.ix_(rows, partner)] = n1
+                            tile = apply_reg_pair(tile, lay, R, W, lane, warp, reg, tpos, ok_t, ok_j, kind, mm)
                     else:
                         if tpos >= 64:
                             bv = ((base >> (tpos - 64)) & 1)[:, None] * np.ones((1, 1 << K), dtype=np.int64)

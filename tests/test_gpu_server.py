@@ -1,0 +1,101 @@
+"""Serving mode on the GPU: continuous batching with byte-based admission.
+
+Every served result must equal the same circuit run alone (within the FP32
+tolerance), whatever else ran with it; admission never exceeds the budget;
+a state larger than the budget is refused.
+"""
+import math
+import time
+
+import numpy as np
+import pytest
+
+from oracle import closed_forms as cf
+from simulador_quantico_b200 import workloads as wl
+from tests.helpers import engine_state, fidelity_gap, oracle_state
+
+pytestmark = pytest.mark.gpu
+
+
+def request_mix(seed, count):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        u = rng.random()
+        if u < 0.6:
+            spec = wl.random_layered(int(rng.integers(10, 17)), 4, seed=seed * 1000 + i)
+            mask = 0
+        elif u < 0.9:
+            n = int(rng.integers(10, 17))
+            spec = wl.qft(n, int(rng.integers(1 << n)))
+            mask = (1 << n) - 1
+        else:
+            m = int(rng.integers(8, 13))
+            spec = wl.grover_search(m, int(rng.integers(1 << m)))
+            mask = (1 << m) - 1
+        reqs.append((spec, mask))
+    return reqs
+
+
+def test_served_results_equal_alone(sq):
+    reqs = request_mix(11, 40)
+    srv = sq.Server("f32", budget_bytes=1 << 30, max_inflight=8, keep_states=True)
+    ids = {}
+    for spec, mask in reqs:
+        rid = srv.submit(spec.build(sq.Circuit()), spec.qubits, spec.init_index, mask)
+        ids[rid] = (spec, mask)
+    results = srv.drain(len(reqs))
+    assert all(r["status"] == 0 for r in results)
+    for r in results:
+        spec, mask = ids[r["id"]]
+        got = srv.result_state(r["id"]).download()
+        alone, _ = engine_state(sq, spec, "f32")
+        assert np.abs(got - alone).max() < 1e-6, spec.name
+        want64 = oracle_state(spec, "f64")
+        assert fidelity_gap(got, want64) < 1e-6
+        assert abs(r["norm"] - 1.0) < 1e-4  # FP32 norm drift over ~200 gates, FP64-accumulated
+        if spec.name == "grover":
+            assert r["argmax"] == spec.meta["search_value"]
+        if spec.name == "qft":
+            assert abs(r["pmax"] - 2.0 ** -spec.qubits) < 1e-6  # uniform magnitudes
+        srv.release(r["id"])
+    srv.close()
+
+
+def test_admission_respects_budget(sq):
+    budget = 4 * (8 << 16)  # four 16-qubit FP32 states
+    srv = sq.Server("f32", budget_bytes=budget, max_inflight=16)
+    n = 16
+    for i in range(12):
+        spec = wl.random_layered(n, 6, seed=i)
+        srv.submit(spec.build(sq.Circuit()), n)
+    seen = 0
+    t0 = time.time()
+    while seen < 12 and time.time() - t0 < 60:
+        p = srv.pending()
+        assert p["bytes_in_use"] <= budget
+        assert p["inflight"] <= 4
+        seen += len(srv.poll(wait_ms=1))
+    assert seen == 12
+    srv.close()
+
+
+def test_oversized_request_refused(sq):
+    srv = sq.Server("f64", budget_bytes=1 << 20)
+    spec = wl.hadamard_benchmark(17)  # 2 MiB FP64 state
+    with pytest.raises(sq.HgmError) as e:
+        srv.submit(spec.build(sq.Circuit()), 17)
+    assert e.value.code == 6
+    srv.close()
+
+
+def test_fp64_server_matches_oracle(sq):
+    reqs = request_mix(5, 12)
+    srv = sq.Server("f64", budget_bytes=1 << 30, max_inflight=4, keep_states=True)
+    ids = {srv.submit(spec.build(sq.Circuit()), spec.qubits, spec.init_index, mask): spec for spec, mask in reqs}
+    for r in srv.drain(len(reqs)):
+        spec = ids[r["id"]]
+        got = srv.result_state(r["id"]).download()
+        assert np.abs(got - oracle_state(spec, "f64")).max() < 1e-12
+        srv.release(r["id"])
+    srv.close()
