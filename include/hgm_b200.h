@@ -145,6 +145,20 @@ int hgm_max_abs_diff(hgm_state *a, hgm_state *b, double *out);
 /* Multiplies every amplitude by `scale`. */
 int hgm_scale(hgm_state *s, double scale);
 
+/* Allocation-free FP64 norm: sum |a|^2 of the device state `d_state`
+ * (2^qubits amplitudes of the given precision), written to the device
+ * double `d_out`, queued on `stream` (NULL: the legacy default stream).
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (code inside a framework that owns every allocation, or running
+ * while another thread captures a CUDA graph): it calls no cudaMalloc,
+ * cudaFree or allocating routine and keeps its partial sums in an 18.5 KiB
+ * device array that every GPU loading this library holds until exit.
+ * Limit: 1..34 qubits (HGM_ERR_UNSUPPORTED beyond).  All calls share that
+ * array: calls that overlap on the GPU race and must be serialised.  The
+ * first call on a device looks the array's address up (make it before any
+ * stream capture). */
+int hgm_norm_noalloc(const void *d_state, int qubits, int precision, double *d_out, void *stream);
+
 /* ---- batched mode --------------------------------------------------------- */
 /* Many independent circuits of uneven size run by one persistent kernel that
  * a CUDA graph replays: hgm_batch_add the circuits, hgm_batch_finalize

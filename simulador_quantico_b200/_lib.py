@@ -83,6 +83,7 @@ def _load():
         "hgm_inner": ([vp, vp, P(d), P(d)], i),
         "hgm_max_abs_diff": ([vp, vp, P(d)], i),
         "hgm_scale": ([vp, d], i),
+        "hgm_norm_noalloc": ([vp, i, i, vp, vp], i),
         "hgm_batch_create": ([i, i, P(vp)], i),
         "hgm_batch_free": ([vp], None),
         "hgm_batch_add": ([vp, vp, i, i64, P(i)], i),

@@ -577,6 +577,82 @@ int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *s
     return HGM_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free FP64 norm (hgm_norm_noalloc)
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory: code embedded in a host
+// framework that owns every device allocation (a plugin handed pre-allocated
+// buffers), or code running while a CUDA graph is being captured elsewhere
+// in the process, where a cudaMalloc would be illegal or would synchronise.
+// This variant of the FP64 norm reduction keeps its per-block partial sums in
+// a file-scope device array, so it allocates nothing: the caller passes the
+// state and a device location for the result.
+//
+// Limits and sharing:
+//   * the array holds NOALLOC_PARTIALS = 2*1184 doubles (18.5 KiB) on every
+//     GPU that loads this library, for the life of the process;
+//   * a reduction uses at most 1184 blocks (one partial each), so any state
+//     of 1..34 qubits fits; more qubits are rejected with HGM_ERR_UNSUPPORTED;
+//   * every call shares the array; each call writes every partial it reads
+//     before reading it, so nothing needs clearing, but calls that overlap
+//     on the GPU (different streams, or different host threads) race on it
+//     and must be serialised by the caller;
+//   * the array's device address is looked up once per device, on the first
+//     call with that device current (cudaGetSymbolAddress); make that first
+//     call before any stream capture.
+constexpr int NOALLOC_PARTIALS = 2 * RED_BLOCKS;
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_PARTIALS];
+
+namespace {
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[64] = {};
+}  // namespace
+
+static int noalloc_scratch(double **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return fail(HGM_ERR_UNSUPPORTED, "device %d beyond 64", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = reinterpret_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return HGM_OK;
+}
+
+}  // namespace hgm
+
+using namespace hgm;
+
+extern "C" int hgm_norm_noalloc(const void *d_state, int qubits, int precision, double *d_out, void *stream) {
+    if (!d_state || !d_out) return fail(HGM_ERR_INVALID, "null state or output pointer");
+    if (precision != HGM_F64 && precision != HGM_F32) return fail(HGM_ERR_INVALID, "bad precision");
+    if (qubits < 1 || qubits > 34)
+        return fail(HGM_ERR_UNSUPPORTED, "qubits=%d outside 1..34 (the scratch holds %d block partials)", qubits,
+                    NOALLOC_PARTIALS / 2);
+    double *partials = nullptr;
+    int rc = noalloc_scratch(&partials);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;  // NULL: the legacy default stream
+    const long long N = 1ll << qubits;
+    const unsigned g = grid_for(N);
+    if (precision == HGM_F64)
+        reduce_kernel<double, double, RED_NORM><<<g, RED_THREADS, 0, st>>>((const double2 *)d_state, nullptr, N, 0,
+                                                                            partials);
+    else
+        reduce_kernel<float, float, RED_NORM><<<g, RED_THREADS, 0, st>>>((const float2 *)d_state, nullptr, N, 0,
+                                                                          partials);
+    reduce_final<RED_NORM><<<1, 32, 0, st>>>(partials, (int)g, d_out);
+    count_launch(2);
+    return check("hgm_norm_noalloc launch");
+}
+
+namespace hgm {
 }  // namespace hgm
 
 using namespace hgm;
