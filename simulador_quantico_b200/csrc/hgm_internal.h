@@ -62,7 +62,23 @@ enum DevKind : int32_t {
     K_LAYER = 6,   // one uncontrolled dense gate on every register bit; the
                    // R matrices follow in the next R records (bit 0 first)
     K_LAYER_REAL = 7,  // the same with real matrices
+    K_PHASE_BLOCK = 8, // diagonal gates with at most one control, combined:
+                       // head record (term counts per category in m[] as
+                       // bytes, cm_reg bit 0: a 2^R table follows, cv_reg:
+                       // active categories), then the term records by
+                       // category, then the table
 };
+
+// Phase-block term categories (kernels.cuh apply_phase_block): F multiplies
+// every register; G[b] the registers whose register bit b is 1, H[b] those
+// where it is 0; D[b] a diagonal gate on register bit b (d0 on H[b], d1 on
+// G[b]).  Counts are stored in this order: F, G[0..R-1], H[0..R-1], D[0..R-1].
+constexpr int PB_MAX_R = 5;
+// Terms per phase-block category (the counts are bytes).
+constexpr int PB_TERMS = 255;
+// Phase-block head: cv_reg bit b (b < R) marks register bit b as having
+// G/H/D terms; this bit marks F terms.
+constexpr uint32_t PB_F_ACTIVE = 1u << 16;
 
 // Target location codes inside a phase: 0..R-1 register bit, 8+q thread bit q
 // (lane bits 0..4, warp bits 5..), 64+g a non-tile index bit g.

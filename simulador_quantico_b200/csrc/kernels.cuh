@@ -232,16 +232,25 @@ __device__ __forceinline__ void reg_anti(A2 (&a)[1 << R], const Real (&m)[8], ui
     }
 }
 
+// Controlled swaps select instead of branching: two selects per component
+// are cheaper than a branch per pair.
 template <typename A2, int R, int T, bool CTRL>
 __device__ __forceinline__ void reg_swap(A2 (&a)[1 << R], uint32_t cm, uint32_t cv) {
 #pragma unroll
     for (int r = 0; r < (1 << R); r++) {
         if (r & (1 << T)) continue;
         const int r1 = r | (1 << T);
-        HGM_PAIR_GUARD(r)
-        const A2 x = a[r];
-        a[r] = a[r1];
-        a[r1] = x;
+        const A2 x = a[r], y = a[r1];
+        if (CTRL) {
+            const bool p = ((uint32_t)r & cm) == cv;
+            a[r].x = p ? y.x : x.x;
+            a[r].y = p ? y.y : x.y;
+            a[r1].x = p ? x.x : y.x;
+            a[r1].y = p ? x.y : y.y;
+        } else {
+            a[r] = y;
+            a[r1] = x;
+        }
     }
 }
 
@@ -300,22 +309,176 @@ __device__ __forceinline__ void load_matrix<float>(const float *__restrict__ src
     }
 }
 
-// A full layer: one uncontrolled dense gate on each register bit, applied
-// bit 0 first, in one straight-line block (no per-gate dispatch).
+// A layer: uncontrolled dense gates on a set of register bits (mask),
+// applied bit 0 first, one straight-line block per active bit (a uniform
+// branch skips inactive bits).  Its matrices follow in popcount(mask) records.
 template <typename Real, typename A2, int R, int T, bool REAL>
 struct LayerStep {
-    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats) {
-        Real m[8];
-        load_matrix<Real>(mats[T].m, m);
-        if (REAL) reg_real<Real, A2, R, T, false>(a, m, 0u, 0u);
-        else reg_dense<Real, A2, R, T, false>(a, m, 0u, 0u);
-        LayerStep<Real, A2, R, T + 1, REAL>::run(a, mats);
+    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats, uint32_t mask) {
+        if (mask & (1u << T)) {
+            Real m[8];
+            load_matrix<Real>(mats->m, m);
+            if (REAL) reg_real<Real, A2, R, T, false>(a, m, 0u, 0u);
+            else reg_dense<Real, A2, R, T, false>(a, m, 0u, 0u);
+            mats++;
+        }
+        LayerStep<Real, A2, R, T + 1, REAL>::run(a, mats, mask);
     }
 };
 template <typename Real, typename A2, int R, bool REAL>
 struct LayerStep<Real, A2, R, R, REAL> {
-    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__) {}
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, uint32_t) {}
 };
+
+// Phase block: diagonal gates with at most one control, combined per thread
+// into a scalar f, per-register-bit factors g[b] (bit 1) and h[b] (bit 0) and
+// an optional host-built 2^R table (gates whose target and control are both
+// register bits); each register is then multiplied once per involved bit.
+// A term applies when its controls on non-tile and thread bits hold; a term
+// whose target is not a register bit contributes d1 or d0 according to this
+// thread's value of that bit.
+template <typename Real, typename A2>
+__device__ __forceinline__ A2 load_c(const Real *__restrict__ p);
+template <>
+__device__ __forceinline__ double2 load_c<double, double2>(const double *__restrict__ p) {
+    return __ldg(reinterpret_cast<const double2 *>(p));
+}
+template <>
+__device__ __forceinline__ float2 load_c<float, float2>(const float *__restrict__ p) {
+    return __ldg(reinterpret_cast<const float2 *>(p));
+}
+
+// Hides a pointer's value from the scheduler so the next term's descriptor
+// loads are issued only after this point: without it, ptxas hoists the loads
+// of every unrolled term and runs out of registers.
+template <typename T>
+__device__ __forceinline__ const T *opaque(const T *p) {
+    asm volatile("" : "+l"(p));
+    return p;
+}
+
+template <typename Real, typename A2>
+__device__ __forceinline__ bool term_factor(const DevOp<Real> *__restrict__ t, uint64_t base, uint32_t thr, A2 &f0,
+                                            A2 &f1) {
+    t = opaque(t);
+    const uint2 th = __ldg(reinterpret_cast<const uint2 *>(&t->cm_thr));
+    const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(&t->cm_glob));
+    if ((base & gl.x) != gl.y || (thr & th.x) != th.y) return false;
+    const int tpos = __ldg(&t->tpos);
+    f0 = load_c<Real, A2>(t->m);
+    f1 = load_c<Real, A2>(t->m + 6);
+    if (tpos >= TPOS_THREAD) {  // target outside the registers: pick this thread's entry
+        const int bv = tpos >= TPOS_GLOBAL ? (int)((base >> (tpos - TPOS_GLOBAL)) & 1)
+                                           : (int)((thr >> (tpos - TPOS_THREAD)) & 1);
+        if (bv) f0 = f1;
+    }
+    return true;
+}
+
+template <typename Real, typename A2>
+__device__ __forceinline__ A2 cmul2(A2 a, A2 b) {
+    A2 o;
+    o.x = a.x * b.x - a.y * b.y;
+    o.y = a.x * b.y + a.y * b.x;
+    return o;
+}
+
+// Register bit B of a phase block: when the block marks B active, folds the
+// G[B], H[B] and D[B] terms into g (factor of the registers whose bit B is 1)
+// and h (bit B is 0), starting from `carry` (the block's F factor, handed to
+// the first active bit and reset), and multiplies them into the registers
+// with one sweep.  Inactive bits cost nothing but the pointer step.
+template <typename Real, typename A2, int R, int B>
+struct PhaseBits {
+    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ t,
+                                               const uint8_t *cnt, uint32_t act, A2 &carry, uint64_t base,
+                                               uint32_t thr) {
+        const int ng = cnt[1 + B], nh = cnt[1 + R + B], nd = cnt[1 + 2 * R + B];
+        if (act & (1u << B)) {
+            A2 g = carry, h = carry;
+            carry.x = 1;
+            carry.y = 0;
+#pragma unroll 1
+            for (int i = 0; i < ng; i++) {
+                A2 f0, f1;
+                if (term_factor<Real>(t + i, base, thr, f0, f1)) g = cmul2<Real>(g, f0);
+            }
+#pragma unroll 1
+            for (int i = 0; i < nh; i++) {
+                A2 f0, f1;
+                if (term_factor<Real>(t + ng + i, base, thr, f0, f1)) h = cmul2<Real>(h, f0);
+            }
+#pragma unroll 1
+            for (int i = 0; i < nd; i++) {
+                A2 f0, f1;
+                if (term_factor<Real>(t + ng + nh + i, base, thr, f0, f1)) {
+                    h = cmul2<Real>(h, f0);
+                    g = cmul2<Real>(g, f1);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < (1 << R); r++) a[r] = cmul2<Real>(a[r], ((r >> B) & 1) ? g : h);
+        }
+        PhaseBits<Real, A2, R, B + 1>::run(a, t + ng + nh + nd, cnt, act, carry, base, thr);
+    }
+};
+template <typename Real, typename A2, int R>
+struct PhaseBits<Real, A2, R, R> {
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, const uint8_t *,
+                                               uint32_t, A2 &, uint64_t, uint32_t) {}
+};
+
+// K_PHASE_BLOCK: the F terms fold into one per-thread factor; each active
+// register bit costs one sweep of the registers (PhaseBits); the F factor
+// rides on the first active bit's sweep, or gets a sweep of its own when no
+// bit is active; the thread-independent 2^R table, if any, is one more sweep.
+template <typename Real, typename A2, int R>
+__device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, uint64_t base,
+                                                 uint32_t thr) {
+    const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));
+    const int nrec = (int)hdr.y;  // records after the head
+    const bool has_table = hdr.z & 1u;
+    const uint32_t act = hdr.w;   // active register bits, PB_F_ACTIVE: F terms
+    uint8_t cnt[16];
+    {
+        const uint4 c = __ldg(reinterpret_cast<const uint4 *>(op->m));
+        const uint32_t w[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int k = 0; k < 16; k++) cnt[k] = (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
+    }
+    const DevOp<Real> *__restrict__ t = op + 1;
+    A2 carry;
+    carry.x = 1;
+    carry.y = 0;
+    const int nf = cnt[0];
+#pragma unroll 1
+    for (int i = 0; i < nf; i++) {
+        A2 f0, f1;
+        if (term_factor<Real>(t + i, base, thr, f0, f1)) carry = cmul2<Real>(carry, f0);
+    }
+    PhaseBits<Real, A2, R, 0>::run(a, t + nf, cnt, act, carry, base, thr);
+    if ((act & PB_F_ACTIVE) && !(act & ((1u << R) - 1u))) {
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) a[r] = cmul2<Real>(a[r], carry);
+    }
+    if (has_table) {
+        // 2^R complex factors, four per record, after the terms
+        t += nrec - (1 << R) / 4;
+#pragma unroll
+        for (int q = 0; q < (1 << R) / 4; q++) {
+            Real m[8];
+            load_matrix<Real>(t[q].m, m);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                A2 z;
+                z.x = m[2 * k];
+                z.y = m[2 * k + 1];
+                a[4 * q + k] = cmul2<Real>(a[4 * q + k], z);
+            }
+        }
+    }
+    return 1 + nrec;
+}
 
 // Applies record `op` (and, for a layer, its matrix records); returns the
 // number of records consumed.
@@ -324,13 +487,12 @@ __device__ __forceinline__ int apply_op(A2 (&a)[1 << R], const DevOp<Real> *__re
                                         uint32_t thr) {
     const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));  // kind, tpos, cm_reg, cv_reg
     const int kind = (int)hdr.x, tpos = (int)hdr.y;
-    if (kind == K_LAYER) {
-        LayerStep<Real, A2, R, 0, false>::run(a, op + 1);
-        return 1 + R;
-    }
-    if (kind == K_LAYER_REAL) {
-        LayerStep<Real, A2, R, 0, true>::run(a, op + 1);
-        return 1 + R;
+    if (kind == K_PHASE_BLOCK) return apply_phase_block<Real, A2, R>(a, op, base, thr);
+    if (kind == K_LAYER || kind == K_LAYER_REAL) {
+        const uint32_t mask = hdr.z;  // active register bits
+        if (kind == K_LAYER) LayerStep<Real, A2, R, 0, false>::run(a, op + 1, mask);
+        else LayerStep<Real, A2, R, 0, true>::run(a, op + 1, mask);
+        return 1 + __popc(mask);
     }
     const uint4 th = __ldg(reinterpret_cast<const uint4 *>(op) + 1);                 // cm_thr, cv_thr
     const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(op) + 2);       // cm_glob, cv_glob

@@ -46,6 +46,10 @@ void matmul2(const cplx a[4], const cplx b[4], cplx out[4]) {  // out = a * b
     for (int k = 0; k < 4; k++) out[k] = r[k];
 }
 
+// Merges each gate into the previous gate on the same target with the same
+// controls when nothing touched those qubits in between (one record instead
+// of two: the per-record work of the pass kernel outweighs the arithmetic a
+// cheaper matrix form would save).
 std::vector<SOp> fuse_ops(const std::vector<Op> &ops, bool fuse) {
     std::vector<SOp> out;
     out.reserve(ops.size());
@@ -167,15 +171,110 @@ DevOp<Real> encode(const SOp &o, int layout, int R, int W, const int loc_of[64],
     return d;
 }
 
-// Emits a phase's gates.  Uncontrolled dense gates that cover every
-// register bit of the layout, and that can all move to the front of what is
-// left (each commutes with every other gate before it), become one K_LAYER
-// record followed by their R matrices (register bit 0 first); the rest are
-// emitted one record each, in order.
+// Phase block (K_PHASE_BLOCK): diagonal gates with at most one control that
+// can all move to the front of what is left, combined into per-thread
+// factors (kernels.cuh apply_phase_block).  Returns false when fewer than
+// `min_terms` qualify.
+template <typename Real>
+bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, int layout, int R, int W,
+                      const int loc_of[64], uint64_t tmask, int min_terms, std::vector<DevOp<Real>> &out) {
+    // category lists: 0 = F, 1 + b = G[b], 1 + R + b = H[b], 1 + 2R + b = D[b]
+    std::vector<std::vector<int>> cat(1 + 3 * R);
+    std::vector<cplx> table(size_t(1) << R, cplx(1.0, 0.0));
+    bool has_table = false;
+    std::vector<int> members;
+    uint64_t bn = 0, bd = 0;
+    auto loc_role = [&](int g, Role &rl) -> bool {  // false: not a tile bit
+        if (!((tmask >> g) & 1)) return false;
+        rl = role(layout, R, W, loc_of[g]);
+        return true;
+    };
+    for (int idx : rest) {
+        const SOp &op = ops[idx];
+        bool cand = false;
+        if (op.mc == MC_DIAG && __builtin_popcountll(op.cmask) <= 1 && !conflicts(op, bn, bd)) {
+            Role tr, cr;
+            const bool t_reg = loc_role(op.target, tr) && tr.kind == ROLE_REG;
+            int c_bit = op.cmask ? __builtin_ctzll(op.cmask) : -1;
+            const bool c_reg = c_bit >= 0 && loc_role(c_bit, cr) && cr.kind == ROLE_REG;
+            int k = -1;
+            if (t_reg && (c_reg || c_bit < 0)) {
+                // only register bits: thread-independent, folded into the table
+                const int v = c_bit >= 0 ? (int)((op.cval >> c_bit) & 1) : 0;
+                for (size_t r = 0; r < table.size(); r++)
+                    if (c_bit < 0 || (int)((r >> cr.idx) & 1) == v)
+                        table[r] *= ((r >> tr.idx) & 1) ? op.m[3] : op.m[0];
+                has_table = true;
+                cand = true;
+            } else if (t_reg) {
+                k = 1 + 2 * R + tr.idx;  // D[t]
+            } else if (c_reg) {
+                k = ((op.cval >> c_bit) & 1) ? 1 + cr.idx : 1 + R + cr.idx;  // G[c] / H[c]
+            } else {
+                k = 0;  // F
+            }
+            if (k >= 0 && cat[k].size() < (size_t)PB_TERMS) {
+                cat[k].push_back(idx);
+                cand = true;
+            }
+            if (cand) members.push_back(idx);
+        }
+        if (!cand) {
+            bn |= op.nd();
+            bd |= op.dg();
+        }
+    }
+    if ((int)members.size() < min_terms) return false;
+    DevOp<Real> head;
+    memset(&head, 0, sizeof head);
+    head.kind = K_PHASE_BLOCK;
+    head.cm_reg = has_table ? 1u : 0u;
+    uint8_t counts[16] = {0};
+    int nrec = 0;
+    for (int k = 0; k < 1 + 3 * R; k++) {
+        counts[k] = (uint8_t)cat[k].size();
+        nrec += (int)cat[k].size();
+        if (cat[k].empty()) continue;
+        head.cv_reg |= k == 0 ? PB_F_ACTIVE : 1u << ((k - 1) % R);
+    }
+    const int table_recs = has_table ? (1 << R) / 4 : 0;
+    head.tpos = nrec + table_recs;
+    memcpy(head.m, counts, 16);
+    out.push_back(head);
+    // records in the kernel's walk order: F, then per register bit b: G[b], H[b], D[b]
+    for (int idx : cat[0]) out.push_back(encode<Real>(ops[idx], layout, R, W, loc_of, tmask));
+    for (int b = 0; b < R; b++)
+        for (int k : {1 + b, 1 + R + b, 1 + 2 * R + b})
+            for (int idx : cat[k]) out.push_back(encode<Real>(ops[idx], layout, R, W, loc_of, tmask));
+    for (int q = 0; q < table_recs; q++) {
+        DevOp<Real> rec;
+        memset(&rec, 0, sizeof rec);
+        for (int k = 0; k < 4; k++) {
+            rec.m[2 * k] = (Real)table[4 * q + k].real();
+            rec.m[2 * k + 1] = (Real)table[4 * q + k].imag();
+        }
+        out.push_back(rec);
+    }
+    std::vector<int> keep;
+    for (int idx : rest)
+        if (std::find(members.begin(), members.end(), idx) == members.end()) keep.push_back(idx);
+    rest.swap(keep);
+    return true;
+}
+
+// Emits a phase's gates as a list schedule.  At each step: a phase block if
+// at least three diagonal gates (at most one control each) can move to the
+// front; else a layer -- the uncontrolled dense gates on distinct register
+// bits of the layout that could all move to the front of what is left
+// (cm_reg holds the mask of those bits, their matrices follow, lowest
+// register bit first) -- if there are at least two; else a phase block of
+// two; else the first remaining gate on its own record.
 template <typename Real>
 void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, int R, int W, const int loc_of[64],
                 uint64_t tmask, std::vector<DevOp<Real>> &out) {
-    for (;;) {
+    std::vector<int> keep;
+    while (!rest.empty()) {
+        if (emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 3, out)) continue;
         int slot[8];
         for (int k = 0; k < 8; k++) slot[k] = -1;
         int found = 0;
@@ -199,22 +298,30 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, 
             }
             if (found == R) break;
         }
-        if (found < R) break;
-        DevOp<Real> head;
-        memset(&head, 0, sizeof head);
-        head.kind = all_real ? K_LAYER_REAL : K_LAYER;
-        head.tpos = R;
-        out.push_back(head);
-        std::vector<int> keep;
-        for (int k = 0; k < R; k++) out.push_back(encode<Real>(ops[slot[k]], layout, R, W, loc_of, tmask));
-        for (int idx : rest) {
-            bool member = false;
-            for (int k = 0; k < R; k++) member = member || slot[k] == idx;
-            if (!member) keep.push_back(idx);
+        keep.clear();
+        if (found >= 2) {
+            DevOp<Real> head;
+            memset(&head, 0, sizeof head);
+            head.kind = all_real ? K_LAYER_REAL : K_LAYER;
+            head.tpos = found;
+            for (int k = 0; k < R; k++)
+                if (slot[k] >= 0) head.cm_reg |= 1u << k;
+            out.push_back(head);
+            for (int k = 0; k < R; k++)
+                if (slot[k] >= 0) out.push_back(encode<Real>(ops[slot[k]], layout, R, W, loc_of, tmask));
+            for (int idx : rest) {
+                bool member = false;
+                for (int k = 0; k < R; k++) member = member || slot[k] == idx;
+                if (!member) keep.push_back(idx);
+            }
+        } else if (emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 2, out)) {
+            continue;
+        } else {
+            out.push_back(encode<Real>(ops[rest[0]], layout, R, W, loc_of, tmask));
+            keep.assign(rest.begin() + 1, rest.end());
         }
         rest.swap(keep);
     }
-    for (int idx : rest) out.push_back(encode<Real>(ops[idx], layout, R, W, loc_of, tmask));
 }
 
 template <typename Real>

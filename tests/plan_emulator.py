@@ -35,8 +35,9 @@ def op_dtype(real):
 SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f8", 8)]),
             "<f4": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f4", 8)])}
 
-K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL = range(8)
+K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK = range(9)
 LAYOUT_C, LAYOUT_B, LAYOUT_A, LAYOUT_E = 0, 1, 2, 3
+PB_F_ACTIVE = 1 << 16
 REG_BITS = {"f64": 4, "f32": 5}
 
 
@@ -113,6 +114,58 @@ def apply_reg_pair(tile, lay, R, W, lane, warp, reg, tpos, ok_t, ok_j, kind, mm)
     return tile
 
 
+def _term_factor(t, base, thr):
+    """Per (tile, thread) factor of one phase-block term and whether it applies: arrays [T, nthr]."""
+    m = t["m"].astype(np.float64)
+    d0, d1 = m[0] + 1j * m[1], m[6] + 1j * m[7]
+    ok = ((base & int(t["cm_glob"])) == int(t["cv_glob"]))[:, None] & ((thr & int(t["cm_thr"])) == int(t["cv_thr"]))[None, :]
+    tpos = int(t["tpos"])
+    if tpos >= 64:
+        bv = ((base >> (tpos - 64)) & 1)[:, None] * np.ones_like(thr)[None, :]
+    elif tpos >= 8:
+        bv = np.broadcast_to(((thr >> (tpos - 8)) & 1)[None, :], ok.shape)
+    else:
+        bv = np.zeros(ok.shape, dtype=np.int64)
+    f0 = np.where(bv == 1, d1, d0)
+    return ok, f0, d1
+
+
+def apply_phase_block(tile, recs, i, R, base, thr, reg, T, K):
+    counts = np.frombuffer(recs[i]["m"].tobytes()[:16], dtype=np.uint8)
+    has_table = int(recs[i]["cm_reg"]) & 1
+    act = int(recs[i]["cv_reg"])  # active register bits; PB_F_ACTIVE: F terms
+    j = i + 1
+    f = np.ones((T, 1 << K), dtype=np.complex128)
+    for _ in range(int(counts[0])):
+        ok, f0, _d1 = _term_factor(recs[j], base, thr)
+        if act & PB_F_ACTIVE:
+            f = np.where(ok, f * f0, f)
+        j += 1
+    for b in range(R):
+        bit = ((reg >> b) & 1)[None, :]
+        for kind, cnt in (("G", counts[1 + b]), ("H", counts[1 + R + b]), ("D", counts[1 + 2 * R + b])):
+            for _ in range(int(cnt)):
+                if not (act >> b) & 1:  # the kernel skips an inactive bit's terms
+                    j += 1
+                    continue
+                ok, f0, d1 = _term_factor(recs[j], base, thr)
+                if kind == "G":
+                    fac = np.where(bit == 1, f0, 1.0)
+                elif kind == "H":
+                    fac = np.where(bit == 0, f0, 1.0)
+                else:
+                    fac = np.where(bit == 1, d1, f0)
+                f = np.where(ok, f * fac, f)
+                j += 1
+    if has_table:
+        tab = []
+        for q in range((1 << R) // 4):
+            m = recs[j + q]["m"].astype(np.float64)
+            tab += list(m[0::2] + 1j * m[1::2])
+        f = f * np.asarray(tab)[reg][None, :]
+    return tile * f
+
+
 def run(plan, precision, state, iterations=1):
     e = export(plan, precision)
     n = plan.qubits
@@ -148,14 +201,23 @@ def run(plan, precision, state, iterations=1):
                 i = 0
                 while i < len(recs):
                     o = recs[i]
+                    if int(o["kind"]) == K_PHASE_BLOCK:
+                        tile = apply_phase_block(tile, recs, i, R, base, thr, reg, T, K)
+                        i += 1 + int(o["tpos"])
+                        continue
                     if int(o["kind"]) in (K_LAYER, K_LAYER_REAL):
-                        # R uncontrolled dense gates, register bit 0 first
+                        # uncontrolled dense gates on the register bits of the mask, lowest first
+                        mask = int(o["cm_reg"])
+                        k = 0
                         for t in range(R):
-                            mm = recs[i + 1 + t]["m"].astype(np.float64)
+                            if not (mask >> t) & 1:
+                                continue
+                            mm = recs[i + 1 + k]["m"].astype(np.float64)
                             mm = mm[0::2] + 1j * mm[1::2]
                             tile = apply_reg_pair(tile, lay, R, W, lane, warp, reg, t, np.ones(T, bool),
                                                   np.ones(1 << K, bool), K_DENSE, mm)
-                        i += 1 + R
+                            k += 1
+                        i += 1 + k
                         continue
                     i += 1
                     m = o["m"].astype(np.float64)

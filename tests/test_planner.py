@@ -66,6 +66,28 @@ def test_plan_pass_counts():
     assert s["passes"] <= 4 * 3
 
 
+def test_fusion_merges_adjacent():
+    """Adjacent gates on one target merge (H.H and Rz.Rz.Ry become one
+    record each); a gate on another qubit in between does not block it."""
+    h = np.array([[1, 1], [1, -1]]) / np.sqrt(2)
+
+    def rz(t):
+        return np.diag([np.exp(-0.5j * t), np.exp(0.5j * t)])
+
+    def ry(t):
+        return np.array([[np.cos(t / 2), -np.sin(t / 2)], [np.sin(t / 2), np.cos(t / 2)]])
+
+    c = sq.Circuit()
+    c.append_op(0, 0, 0, h)
+    c.append_op(3, 0, 0, h)
+    c.append_op(0, 0, 0, h)
+    assert sq.Plan(c, 12, "f64").stats()["ops"] == 2
+    c = sq.Circuit()
+    for m in (rz(0.3), rz(0.5), ry(0.7)):
+        c.append_op(0, 0, 0, m)
+    assert sq.Plan(c, 12, "f64").stats()["ops"] == 1
+
+
 def test_grover_plan_fast():
     """The unrolled 27-qubit Grover (grover.out 27, ~682k PTs) plans in seconds."""
     import time
