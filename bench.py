@@ -174,7 +174,7 @@ def run_timed(dist, sq, step, steps, warmup):
 def workload_layered(args, dist, sq):
     from simulador_quantico_b200 import workloads as wl
 
-    n, layers, prec = args.qubits or 30, args.layers or 40, "f64"
+    n, layers, prec = args.qubits or 30, args.layers or 40, args.precision
     spec = wl.random_layered(n, layers, seed=2024)
     c = spec.build(sq.Circuit())
     plan = sq.Plan(c, n, prec)
@@ -197,12 +197,14 @@ def workload_layered(args, dist, sq):
     e2e = e2e_layered(dist, sq, spec, n, prec) if not args.skip_e2e else None
     st.free()
     line = base_line(args, dist, "gate-layers/s (30q random Rz/Ry+CNOT layers)", value, "layers/s", ms_step,
-                     "f64", {"workload": f"layered-{n}q-{layers}layers", "qubits": n, "layers": layers, "precision": "fp64",
-                             "state_bytes": S, "passes_per_step": stats["passes"], "ops_after_fusion": stats["ops"],
-                             "l2": "state 16 GiB >> 126 MB L2, no flush needed"})
+                     prec, {"workload": f"layered-{n}q-{layers}layers", "qubits": n, "layers": layers,
+                            "precision": {"f64": "fp64", "f32": "fp32"}[prec],
+                            "state_bytes": S, "passes_per_step": stats["passes"], "ops_after_fusion": stats["ops"],
+                            "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"})
     line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
-                        "kernel": "pass_kernel<double,%d,%d>" % (stats["reg_bits"], stats["warp_bits"]),
+                        "kernel": "pass_kernel<%s,%d,%d>" % ({"f64": "double", "f32": "float"}[prec], stats["reg_bits"],
+                                                             stats["warp_bits"]),
                         "algorithmic_bytes_per_launch": 2 * S}
     line["gpu_launches"] = launches
     line["clocks"] = clk.summary()
@@ -217,7 +219,7 @@ def e2e_layered(dist, sq, spec, n, prec):
     L.setDevice(dist.local_rank)
     c = spec.build(sq.Circuit())
     pts = c.ref_pts(prec)
-    host = np.zeros(1 << n, dtype=np.complex128)
+    host = np.zeros(1 << n, dtype=np.complex64 if prec == "f32" else np.complex128)
     host[0] = 1.0
     t0 = time.perf_counter()
     L.GpuExecutionWrapper(host.ctypes.data, pts, n, 4, 8, 1, 64, 2, 1)
@@ -527,6 +529,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--qubits", type=int, default=0, help="override the workload's qubit count (profiling runs)")
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")
     args = ap.parse_args()
     args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
                         "served": SERVED_METRIC}.get(args.workload, args.workload)

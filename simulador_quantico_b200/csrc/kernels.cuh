@@ -42,12 +42,15 @@
 namespace hgm {
 
 // Register budget per thread.  The FP32 tile (32 float2) and the FP64 tile
-// (16 double2) both hold 64 data registers.
+// (16 double2) both hold 64 data registers.  128 lets 4 CTAs of 4 warps share
+// an SM; the pass kernel is latency-bound, and the fourth CTA outweighs the
+// spills the cap brings (26-qubit layered passes: FP64 -13%, FP32 -2%, QFT
+// -12% against a 168-register cap with 3 CTAs per SM).
 #ifndef HGM_MAXREG_F32
-#define HGM_MAXREG_F32 168
+#define HGM_MAXREG_F32 128
 #endif
 #ifndef HGM_MAXREG_F64
-#define HGM_MAXREG_F64 168
+#define HGM_MAXREG_F64 128
 #endif
 // Shared-memory carveout for the pass kernels, in percent (-1: driver's
 // choice).  The L1 left over holds the loads in flight; forcing the maximum
@@ -146,6 +149,61 @@ struct StoreF {
     }
 };
 
+// ---- in-place amplitude updates --------------------------------------------
+// Every update of a register amplitude goes through these inline-PTX
+// primitives.  Their amplitude operands are tied ("+"), so each result is
+// written into the register that held the input and the amplitudes keep their
+// registers from one gate to the next.  Written as plain expressions, the
+// compiler left each result in a fresh register and copied it back wherever
+// the op loop's dispatch paths merge; those copies outnumbered the
+// floating-point instructions of the pass kernel.  Negated coefficients come
+// in as operands (PTX fma has no negated-operand form).
+#define HGM_INPLACE_PRIMITIVES(REAL, SFX, C)                                                                      \
+    /* (x, y) <- M (x, y), complex M = m[0..7] (row-major re/im), n_k = -m_k */                                 \
+    __device__ __forceinline__ void ip_dense(REAL &xr, REAL &xi, REAL &yr, REAL &yi, const REAL(&m)[8], REAL n1, \
+                                             REAL n3, REAL n5, REAL n7) {                                        \
+        asm("{\n\t.reg ." SFX " t0, t1, t2, t3;\n\t"                                                              \
+            "mul.rn." SFX " t0, %4, %0;\n\tmul.rn." SFX " t1, %4, %1;\n\t"                                          \
+            "mul.rn." SFX " t2, %8, %0;\n\tmul.rn." SFX " t3, %8, %1;\n\t"                                          \
+            "fma.rn." SFX " t0, %12, %1, t0;\n\tfma.rn." SFX " t1, %5, %0, t1;\n\t"                                 \
+            "fma.rn." SFX " t2, %14, %1, t2;\n\tfma.rn." SFX " t3, %9, %0, t3;\n\t"                                 \
+            "fma.rn." SFX " t0, %6, %2, t0;\n\tfma.rn." SFX " t1, %7, %2, t1;\n\t"                                  \
+            "fma.rn." SFX " t2, %10, %2, t2;\n\tfma.rn." SFX " t3, %11, %2, t3;\n\t"                                \
+            "fma.rn." SFX " %0, %13, %3, t0;\n\tfma.rn." SFX " %1, %6, %3, t1;\n\t"                                 \
+            "fma.rn." SFX " %2, %15, %3, t2;\n\tfma.rn." SFX " %3, %10, %3, t3;\n\t}"                               \
+            : "+" C(xr), "+" C(xi), "+" C(yr), "+" C(yi)                                                         \
+            : C(m[0]), C(m[1]), C(m[2]), C(m[3]), C(m[4]), C(m[5]), C(m[6]), C(m[7]), C(n1), C(n3), C(n5),      \
+              C(n7));                                                                                            \
+    }                                                                                                            \
+    /* (x, y) <- M (x, y), real M = (m00, m01, m10, m11) */                                                      \
+    __device__ __forceinline__ void ip_real(REAL &xr, REAL &xi, REAL &yr, REAL &yi, REAL m00, REAL m01,         \
+                                            REAL m10, REAL m11) {                                                \
+        asm("{\n\t.reg ." SFX " t0, t1, t2, t3;\n\t"                                                              \
+            "mul.rn." SFX " t0, %4, %0;\n\tmul.rn." SFX " t1, %6, %0;\n\t"                                          \
+            "mul.rn." SFX " t2, %4, %1;\n\tmul.rn." SFX " t3, %6, %1;\n\t"                                          \
+            "fma.rn." SFX " %0, %5, %2, t0;\n\tfma.rn." SFX " %2, %7, %2, t1;\n\t"                                  \
+            "fma.rn." SFX " %1, %5, %3, t2;\n\tfma.rn." SFX " %3, %7, %3, t3;\n\t}"                                 \
+            : "+" C(xr), "+" C(xi), "+" C(yr), "+" C(yi)                                                         \
+            : C(m00), C(m01), C(m10), C(m11));                                                                   \
+    }                                                                                                            \
+    /* x <- x * (fr + i fi), nfi = -fi */                                                                        \
+    __device__ __forceinline__ void ip_cmul(REAL &xr, REAL &xi, REAL fr, REAL fi, REAL nfi) {                  \
+        asm("{\n\t.reg ." SFX " t0, t1;\n\t"                                                                      \
+            "mul.rn." SFX " t0, %2, %0;\n\tmul.rn." SFX " t1, %3, %0;\n\t"                                          \
+            "fma.rn." SFX " %0, %4, %1, t0;\n\tfma.rn." SFX " %1, %2, %1, t1;\n\t}"                                 \
+            : "+" C(xr), "+" C(xi)                                                                               \
+            : C(fr), C(fi), C(nfi));                                                                             \
+    }
+HGM_INPLACE_PRIMITIVES(double, "f64", "d")
+HGM_INPLACE_PRIMITIVES(float, "f32", "f")
+#undef HGM_INPLACE_PRIMITIVES
+
+// amplitude a <- a * f (complex factor f)
+template <typename A2>
+__device__ __forceinline__ void ip_cmul2(A2 &a, A2 f) {
+    ip_cmul(a.x, a.y, f.x, f.y, -f.y);
+}
+
 // ---- gate application on register bits -----------------------------------
 
 template <typename Real, typename A2>
@@ -166,19 +224,13 @@ __device__ __forceinline__ A2 cmul(A2 a, Real mr, Real mi) {
 
 template <typename Real, typename A2, int R, int T, bool CTRL>
 __device__ __forceinline__ void reg_dense(A2 (&a)[1 << R], const Real (&m)[8], uint32_t cm, uint32_t cv) {
+    const Real n1 = -m[1], n3 = -m[3], n5 = -m[5], n7 = -m[7];
 #pragma unroll
     for (int r = 0; r < (1 << R); r++) {
         if (r & (1 << T)) continue;
         const int r1 = r | (1 << T);
         HGM_PAIR_GUARD(r)
-        const A2 x = a[r], y = a[r1];
-        A2 o0, o1;
-        o0.x = m[0] * x.x - m[1] * x.y + m[2] * y.x - m[3] * y.y;
-        o0.y = m[0] * x.y + m[1] * x.x + m[2] * y.y + m[3] * y.x;
-        o1.x = m[4] * x.x - m[5] * x.y + m[6] * y.x - m[7] * y.y;
-        o1.y = m[4] * x.y + m[5] * x.x + m[6] * y.y + m[7] * y.x;
-        a[r] = o0;
-        a[r1] = o1;
+        ip_dense(a[r].x, a[r].y, a[r1].x, a[r1].y, m, n1, n3, n5, n7);
     }
 }
 
@@ -189,33 +241,29 @@ __device__ __forceinline__ void reg_real(A2 (&a)[1 << R], const Real (&m)[8], ui
         if (r & (1 << T)) continue;
         const int r1 = r | (1 << T);
         HGM_PAIR_GUARD(r)
-        const A2 x = a[r], y = a[r1];
-        A2 o0, o1;
-        o0.x = m[0] * x.x + m[2] * y.x;
-        o0.y = m[0] * x.y + m[2] * y.y;
-        o1.x = m[4] * x.x + m[6] * y.x;
-        o1.y = m[4] * x.y + m[6] * y.y;
-        a[r] = o0;
-        a[r1] = o1;
+        ip_real(a[r].x, a[r].y, a[r1].x, a[r1].y, m[0], m[2], m[4], m[6]);
     }
 }
 
 template <typename Real, typename A2, int R, int T, bool CTRL>
 __device__ __forceinline__ void reg_diag(A2 (&a)[1 << R], const Real (&m)[8], uint32_t cm, uint32_t cv) {
+    const Real n1 = -m[1], n7 = -m[7];
 #pragma unroll
     for (int r = 0; r < (1 << R); r++) {
         HGM_PAIR_GUARD(r)
-        a[r] = (r & (1 << T)) ? cmul<Real>(a[r], m[6], m[7]) : cmul<Real>(a[r], m[0], m[1]);
+        if (r & (1 << T)) ip_cmul(a[r].x, a[r].y, m[6], m[7], n7);
+        else ip_cmul(a[r].x, a[r].y, m[0], m[1], n1);
     }
 }
 
 template <typename Real, typename A2, int R, int T, bool CTRL>
 __device__ __forceinline__ void reg_phase(A2 (&a)[1 << R], const Real (&m)[8], uint32_t cm, uint32_t cv) {
+    const Real n7 = -m[7];
 #pragma unroll
     for (int r = 0; r < (1 << R); r++) {
         if (!(r & (1 << T))) continue;
         HGM_PAIR_GUARD(r)
-        a[r] = cmul<Real>(a[r], m[6], m[7]);
+        ip_cmul(a[r].x, a[r].y, m[6], m[7], n7);
     }
 }
 
@@ -258,31 +306,70 @@ __device__ __forceinline__ void reg_swap(A2 (&a)[1 << R], uint32_t cm, uint32_t 
 // same for all of a thread's registers that satisfy the register controls.
 template <typename Real, typename A2, int R, bool CTRL>
 __device__ __forceinline__ void reg_scale(A2 (&a)[1 << R], Real fr, Real fi, uint32_t cm, uint32_t cv) {
+    const Real nfi = -fi;
 #pragma unroll
     for (int r = 0; r < (1 << R); r++) {
         HGM_PAIR_GUARD(r)
-        a[r] = cmul<Real>(a[r], fr, fi);
+        ip_cmul(a[r].x, a[r].y, fr, fi, nfi);
     }
 }
+
+// Kind dispatch as a chain of independent bit tests (not a switch): each
+// body updates the registers in place and merges with the path that skips
+// it, the shape under which the registers keep their places (a switch here
+// became a jump table and cost a hundred register copies per gate).
+template <typename Real>
+__device__ __forceinline__ void load_matrix(const Real *__restrict__ src, Real (&m)[8]);
 
 template <typename Real, typename A2, int R, int T, bool CTRL>
-__device__ __forceinline__ void reg_kind_c(int kind, A2 (&a)[1 << R], const Real (&m)[8], uint32_t cm,
+__device__ __forceinline__ void reg_kind_c(uint32_t kbit, A2 (&a)[1 << R], const Real *__restrict__ mp, uint32_t cm,
                                            uint32_t cv) {
-    switch (kind) {
-        case K_DENSE: reg_dense<Real, A2, R, T, CTRL>(a, m, cm, cv); break;
-        case K_REAL: reg_real<Real, A2, R, T, CTRL>(a, m, cm, cv); break;
-        case K_DIAG: reg_diag<Real, A2, R, T, CTRL>(a, m, cm, cv); break;
-        case K_PHASE: reg_phase<Real, A2, R, T, CTRL>(a, m, cm, cv); break;
-        case K_ANTI: reg_anti<Real, A2, R, T, CTRL>(a, m, cm, cv); break;
-        default: reg_swap<A2, R, T, CTRL>(a, cm, cv); break;
+    // each body loads its own matrix, so no matrix is live across the chain
+    if (kbit & (1u << K_DENSE)) {
+        Real m[8];
+        load_matrix<Real>(mp, m);
+        reg_dense<Real, A2, R, T, CTRL>(a, m, cm, cv);
     }
+    if (kbit & (1u << K_REAL)) {
+        Real m[8];
+        load_matrix<Real>(mp, m);
+        reg_real<Real, A2, R, T, CTRL>(a, m, cm, cv);
+    }
+    if (kbit & (1u << K_DIAG)) {
+        Real m[8];
+        load_matrix<Real>(mp, m);
+        reg_diag<Real, A2, R, T, CTRL>(a, m, cm, cv);
+    }
+    if (kbit & (1u << K_PHASE)) {
+        Real m[8];
+        load_matrix<Real>(mp, m);
+        reg_phase<Real, A2, R, T, CTRL>(a, m, cm, cv);
+    }
+    if (kbit & (1u << K_ANTI)) {
+        Real m[8];
+        load_matrix<Real>(mp, m);
+        reg_anti<Real, A2, R, T, CTRL>(a, m, cm, cv);
+    }
+    if (kbit & (1u << K_SWAP)) reg_swap<A2, R, T, CTRL>(a, cm, cv);
 }
 
+// Target dispatch, the same way: one bit test per register bit.
 template <typename Real, typename A2, int R, int T>
-__device__ __forceinline__ void reg_kind(int kind, A2 (&a)[1 << R], const Real (&m)[8], uint32_t cm, uint32_t cv) {
-    if (cm == 0) reg_kind_c<Real, A2, R, T, false>(kind, a, m, cm, cv);
-    else reg_kind_c<Real, A2, R, T, true>(kind, a, m, cm, cv);
-}
+struct RegTarget {
+    __device__ __forceinline__ static void run(uint32_t tbit, uint32_t kbit, A2 (&a)[1 << R],
+                                               const Real *__restrict__ mp, uint32_t cm, uint32_t cv) {
+        if (tbit & (1u << T)) {
+            if (cm == 0) reg_kind_c<Real, A2, R, T, false>(kbit, a, mp, cm, cv);
+            else reg_kind_c<Real, A2, R, T, true>(kbit, a, mp, cm, cv);
+        }
+        RegTarget<Real, A2, R, T + 1>::run(tbit, kbit, a, mp, cm, cv);
+    }
+};
+template <typename Real, typename A2, int R>
+struct RegTarget<Real, A2, R, R> {
+    __device__ __forceinline__ static void run(uint32_t, uint32_t, A2 (&)[1 << R], const Real *__restrict__,
+                                               uint32_t, uint32_t) {}
+};
 
 template <typename Real>
 __device__ __forceinline__ void load_matrix(const Real *__restrict__ src, Real (&m)[8]);
@@ -417,7 +504,7 @@ struct PhaseBits {
                 }
             }
 #pragma unroll
-            for (int r = 0; r < (1 << R); r++) a[r] = cmul2<Real>(a[r], ((r >> B) & 1) ? g : h);
+            for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], ((r >> B) & 1) ? g : h);
         }
         PhaseBits<Real, A2, R, B + 1>::run(a, t + ng + nh + nd, cnt, act, carry, base, thr);
     }
@@ -459,7 +546,7 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
     PhaseBits<Real, A2, R, 0>::run(a, t + nf, cnt, act, carry, base, thr);
     if ((act & PB_F_ACTIVE) && !(act & ((1u << R) - 1u))) {
 #pragma unroll
-        for (int r = 0; r < (1 << R); r++) a[r] = cmul2<Real>(a[r], carry);
+        for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], carry);
     }
     if (has_table) {
         // 2^R complex factors, four per record, after the terms
@@ -470,10 +557,7 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
             load_matrix<Real>(t[q].m, m);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                A2 z;
-                z.x = m[2 * k];
-                z.y = m[2 * k + 1];
-                a[4 * q + k] = cmul2<Real>(a[4 * q + k], z);
+                ip_cmul(a[4 * q + k].x, a[4 * q + k].y, m[2 * k], m[2 * k + 1], -m[2 * k + 1]);
             }
         }
     }
@@ -499,22 +583,16 @@ __device__ __forceinline__ int apply_op(A2 (&a)[1 << R], const DevOp<Real> *__re
     if ((base & gl.x) != gl.y) return 1;
     if ((thr & th.x) != th.y) return 1;
     const uint32_t cm = hdr.z, cv = hdr.w;
-    Real m[8];
-    load_matrix<Real>(op->m, m);
     if (tpos < R) {
-        switch (tpos) {
-            case 0: reg_kind<Real, A2, R, 0>(kind, a, m, cm, cv); return 1;
-            case 1: reg_kind<Real, A2, R, 1>(kind, a, m, cm, cv); return 1;
-            case 2: reg_kind<Real, A2, R, 2>(kind, a, m, cm, cv); return 1;
-            case 3: reg_kind<Real, A2, R, 3>(kind, a, m, cm, cv); return 1;
-            default: reg_kind<Real, A2, R, (R > 4 ? 4 : 3)>(kind, a, m, cm, cv); return 1;
-        }
+        RegTarget<Real, A2, R, 0>::run(1u << tpos, 1u << kind, a, op->m, cm, cv);
+        return 1;
     }
     // diagonal gate on a thread bit or a non-tile index bit
     const int bv = tpos >= TPOS_GLOBAL ? (int)((base >> (tpos - TPOS_GLOBAL)) & 1)
                                        : (int)((thr >> (tpos - TPOS_THREAD)) & 1);
     if (kind == K_PHASE && !bv) return 1;
-    const Real fr = bv ? m[6] : m[0], fi = bv ? m[7] : m[1];
+    const A2 f = load_c<Real, A2>(op->m + (bv ? 6 : 0));
+    const Real fr = f.x, fi = f.y;
     if (cm == 0) reg_scale<Real, A2, R, false>(a, fr, fi, cm, cv);
     else reg_scale<Real, A2, R, true>(a, fr, fi, cm, cv);
     return 1;

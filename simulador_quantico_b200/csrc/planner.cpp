@@ -268,7 +268,7 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, int l
 // bits of the layout that could all move to the front of what is left
 // (cm_reg holds the mask of those bits, their matrices follow, lowest
 // register bit first) -- if there are at least two; else a phase block of
-// two; else the first remaining gate on its own record.
+// two; else a layer of one; else the first remaining gate on its own record.
 template <typename Real>
 void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, int R, int W, const int loc_of[64],
                 uint64_t tmask, std::vector<DevOp<Real>> &out) {
@@ -299,7 +299,16 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, 
             if (found == R) break;
         }
         keep.clear();
-        if (found >= 2) {
+        // a lone dense gate goes out as a one-gate layer (the cheaper
+        // dispatch) when it is the first remaining gate and no phase block of
+        // two is available; otherwise the first gate goes out on its own so
+        // that a wider layer can still form behind it
+        bool lone = false;
+        if (found == 1) {
+            if (emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 2, out)) continue;
+            for (int k = 0; k < R; k++) lone = lone || slot[k] == rest[0];
+        }
+        if (found >= 2 || lone) {
             DevOp<Real> head;
             memset(&head, 0, sizeof head);
             head.kind = all_real ? K_LAYER_REAL : K_LAYER;
@@ -314,7 +323,7 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, 
                 for (int k = 0; k < R; k++) member = member || slot[k] == idx;
                 if (!member) keep.push_back(idx);
             }
-        } else if (emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 2, out)) {
+        } else if (found != 1 && emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 2, out)) {
             continue;
         } else {
             out.push_back(encode<Real>(ops[rest[0]], layout, R, W, loc_of, tmask));
