@@ -138,14 +138,18 @@ struct LoadF {
         a[r] = __ldcg(p + reg_offset<R, r>(rs));
     }
 };
+// Register r goes to element idx ^ offset(r): idx already carries the
+// offset of the relabeling mask (the offsets are disjoint bits, so
+// offset(r ^ xr) = offset(r) ^ offset(xr)).
 template <typename A2, int R>
 struct StoreF {
     const A2 (&a)[1 << R];
     A2 *__restrict__ p;
+    uint64_t idx;
     const uint64_t (&rs)[R];
     template <int r>
     __device__ __forceinline__ void go() {
-        __stcg(p + reg_offset<R, r>(rs), a[r]);
+        __stcg(p + (idx ^ reg_offset<R, r>(rs)), a[r]);
     }
 };
 
@@ -320,24 +324,28 @@ __device__ __forceinline__ void reg_scale(A2 (&a)[1 << R], Real fr, Real fi, uin
 // became a jump table and cost a hundred register copies per gate).
 template <typename Real>
 __device__ __forceinline__ void load_matrix(const Real *__restrict__ src, Real (&m)[8]);
+template <typename Real>
+__device__ __forceinline__ void load_matrix_flip(const Real *__restrict__ src, Real (&m)[8], bool flip);
+template <typename Real, typename A2>
+__device__ __forceinline__ A2 load_c(const Real *__restrict__ p);
 
 template <typename Real, typename A2, int R, int T, bool CTRL>
 __device__ __forceinline__ void reg_kind_c(uint32_t kbit, A2 (&a)[1 << R], const Real *__restrict__ mp, uint32_t cm,
-                                           uint32_t cv) {
+                                           uint32_t cv, bool flip) {
     // each body loads its own matrix, so no matrix is live across the chain
     if (kbit & (1u << K_DENSE)) {
         Real m[8];
-        load_matrix<Real>(mp, m);
+        load_matrix_flip<Real>(mp, m, flip);
         reg_dense<Real, A2, R, T, CTRL>(a, m, cm, cv);
     }
     if (kbit & (1u << K_REAL)) {
         Real m[8];
-        load_matrix<Real>(mp, m);
+        load_matrix_flip<Real>(mp, m, flip);
         reg_real<Real, A2, R, T, CTRL>(a, m, cm, cv);
     }
     if (kbit & (1u << K_DIAG)) {
         Real m[8];
-        load_matrix<Real>(mp, m);
+        load_matrix_flip<Real>(mp, m, flip);
         reg_diag<Real, A2, R, T, CTRL>(a, m, cm, cv);
     }
     if (kbit & (1u << K_PHASE)) {
@@ -347,7 +355,7 @@ __device__ __forceinline__ void reg_kind_c(uint32_t kbit, A2 (&a)[1 << R], const
     }
     if (kbit & (1u << K_ANTI)) {
         Real m[8];
-        load_matrix<Real>(mp, m);
+        load_matrix_flip<Real>(mp, m, flip);
         reg_anti<Real, A2, R, T, CTRL>(a, m, cm, cv);
     }
     if (kbit & (1u << K_SWAP)) reg_swap<A2, R, T, CTRL>(a, cm, cv);
@@ -357,18 +365,18 @@ __device__ __forceinline__ void reg_kind_c(uint32_t kbit, A2 (&a)[1 << R], const
 template <typename Real, typename A2, int R, int T>
 struct RegTarget {
     __device__ __forceinline__ static void run(uint32_t tbit, uint32_t kbit, A2 (&a)[1 << R],
-                                               const Real *__restrict__ mp, uint32_t cm, uint32_t cv) {
+                                               const Real *__restrict__ mp, uint32_t cm, uint32_t cv, bool flip) {
         if (tbit & (1u << T)) {
-            if (cm == 0) reg_kind_c<Real, A2, R, T, false>(kbit, a, mp, cm, cv);
-            else reg_kind_c<Real, A2, R, T, true>(kbit, a, mp, cm, cv);
+            if (cm == 0) reg_kind_c<Real, A2, R, T, false>(kbit, a, mp, cm, cv, flip);
+            else reg_kind_c<Real, A2, R, T, true>(kbit, a, mp, cm, cv, flip);
         }
-        RegTarget<Real, A2, R, T + 1>::run(tbit, kbit, a, mp, cm, cv);
+        RegTarget<Real, A2, R, T + 1>::run(tbit, kbit, a, mp, cm, cv, flip);
     }
 };
 template <typename Real, typename A2, int R>
 struct RegTarget<Real, A2, R, R> {
     __device__ __forceinline__ static void run(uint32_t, uint32_t, A2 (&)[1 << R], const Real *__restrict__,
-                                               uint32_t, uint32_t) {}
+                                               uint32_t, uint32_t, bool) {}
 };
 
 template <typename Real>
@@ -396,25 +404,42 @@ __device__ __forceinline__ void load_matrix<float>(const float *__restrict__ src
     }
 }
 
+// Loads a gate matrix; with `flip` set, the matrix with both bit values of
+// its target exchanged (X M X: m00 <-> m11, m01 <-> m10), for registers whose
+// labels have that bit swapped (register relabeling, below).
+template <typename Real>
+__device__ __forceinline__ void load_matrix_flip(const Real *__restrict__ src, Real (&m)[8], bool flip) {
+    // entry k of the swapped matrix is entry 3 - k = k ^ 3 of the stored one
+    const int fx = flip ? 3 : 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const typename V2<Real>::T v = load_c<Real, typename V2<Real>::T>(src + 2 * (k ^ fx));
+        m[2 * k] = v.x;
+        m[2 * k + 1] = v.y;
+    }
+}
+
 // A layer: uncontrolled dense gates on a set of register bits (mask),
 // applied bit 0 first, one straight-line block per active bit (a uniform
 // branch skips inactive bits).  Its matrices follow in popcount(mask) records.
 template <typename Real, typename A2, int R, int T, bool REAL>
 struct LayerStep {
-    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats, uint32_t mask) {
+    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats, uint32_t mask,
+                                               uint32_t xr) {
         if (mask & (1u << T)) {
             Real m[8];
-            load_matrix<Real>(mats->m, m);
+            load_matrix_flip<Real>(mats->m, m, (xr >> T) & 1u);
             if (REAL) reg_real<Real, A2, R, T, false>(a, m, 0u, 0u);
             else reg_dense<Real, A2, R, T, false>(a, m, 0u, 0u);
             mats++;
         }
-        LayerStep<Real, A2, R, T + 1, REAL>::run(a, mats, mask);
+        LayerStep<Real, A2, R, T + 1, REAL>::run(a, mats, mask, xr);
     }
 };
 template <typename Real, typename A2, int R, bool REAL>
 struct LayerStep<Real, A2, R, R, REAL> {
-    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, uint32_t) {}
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, uint32_t,
+                                               uint32_t) {}
 };
 
 // Phase block: diagonal gates with at most one control, combined per thread
@@ -470,6 +495,13 @@ __device__ __forceinline__ A2 cmul2(A2 a, A2 b) {
     return o;
 }
 
+// Byte K of the 16 phase-block term counts, kept packed in four words.
+template <int K>
+__device__ __forceinline__ int count_byte(const uint4 &c) {
+    const uint32_t w = K < 4 ? c.x : K < 8 ? c.y : K < 12 ? c.z : c.w;
+    return (int)((w >> (8 * (K & 3))) & 0xffu);
+}
+
 // Register bit B of a phase block: when the block marks B active, folds the
 // G[B], H[B] and D[B] terms into g (factor of the registers whose bit B is 1)
 // and h (bit B is 0), starting from `carry` (the block's F factor, handed to
@@ -478,9 +510,9 @@ __device__ __forceinline__ A2 cmul2(A2 a, A2 b) {
 template <typename Real, typename A2, int R, int B>
 struct PhaseBits {
     __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ t,
-                                               const uint8_t *cnt, uint32_t act, A2 &carry, uint64_t base,
-                                               uint32_t thr) {
-        const int ng = cnt[1 + B], nh = cnt[1 + R + B], nd = cnt[1 + 2 * R + B];
+                                               const uint4 &cnt, uint32_t act, A2 &carry, uint64_t base,
+                                               uint32_t thr, uint32_t xr) {
+        const int ng = count_byte<1 + B>(cnt), nh = count_byte<1 + R + B>(cnt), nd = count_byte<1 + 2 * R + B>(cnt);
         if (act & (1u << B)) {
             A2 g = carry, h = carry;
             carry.x = 1;
@@ -503,16 +535,19 @@ struct PhaseBits {
                     g = cmul2<Real>(g, f1);
                 }
             }
+            // g belongs to the registers whose label has bit B set
+            const bool flip = (xr >> B) & 1u;
+            const A2 g1 = flip ? h : g, h1 = flip ? g : h;
 #pragma unroll
-            for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], ((r >> B) & 1) ? g : h);
+            for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], ((r >> B) & 1) ? g1 : h1);
         }
-        PhaseBits<Real, A2, R, B + 1>::run(a, t + ng + nh + nd, cnt, act, carry, base, thr);
+        PhaseBits<Real, A2, R, B + 1>::run(a, t + ng + nh + nd, cnt, act, carry, base, thr, xr);
     }
 };
 template <typename Real, typename A2, int R>
 struct PhaseBits<Real, A2, R, R> {
-    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, const uint8_t *,
-                                               uint32_t, A2 &, uint64_t, uint32_t) {}
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, const uint4 &,
+                                               uint32_t, A2 &, uint64_t, uint32_t, uint32_t) {}
 };
 
 // K_PHASE_BLOCK: the F terms fold into one per-thread factor; each active
@@ -521,44 +556,37 @@ struct PhaseBits<Real, A2, R, R> {
 // bit is active; the thread-independent 2^R table, if any, is one more sweep.
 template <typename Real, typename A2, int R>
 __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, uint64_t base,
-                                                 uint32_t thr) {
+                                                 uint32_t thr, uint32_t xr) {
     const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));
     const int nrec = (int)hdr.y;  // records after the head
     const bool has_table = hdr.z & 1u;
     const uint32_t act = hdr.w;   // active register bits, PB_F_ACTIVE: F terms
-    uint8_t cnt[16];
-    {
-        const uint4 c = __ldg(reinterpret_cast<const uint4 *>(op->m));
-        const uint32_t w[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-        for (int k = 0; k < 16; k++) cnt[k] = (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
-    }
+    const uint4 cnt = __ldg(reinterpret_cast<const uint4 *>(op->m));  // 16 count bytes
     const DevOp<Real> *__restrict__ t = op + 1;
     A2 carry;
     carry.x = 1;
     carry.y = 0;
-    const int nf = cnt[0];
+    const int nf = count_byte<0>(cnt);
 #pragma unroll 1
     for (int i = 0; i < nf; i++) {
         A2 f0, f1;
         if (term_factor<Real>(t + i, base, thr, f0, f1)) carry = cmul2<Real>(carry, f0);
     }
-    PhaseBits<Real, A2, R, 0>::run(a, t + nf, cnt, act, carry, base, thr);
+    PhaseBits<Real, A2, R, 0>::run(a, t + nf, cnt, act, carry, base, thr, xr);
     if ((act & PB_F_ACTIVE) && !(act & ((1u << R) - 1u))) {
 #pragma unroll
         for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], carry);
     }
     if (has_table) {
-        // 2^R complex factors, four per record, after the terms
+        // 2^R complex factors by register label, four per record, after the
+        // terms; register r holds label r ^ xr
         t += nrec - (1 << R) / 4;
+        const Real *__restrict__ z = t->m;
 #pragma unroll
-        for (int q = 0; q < (1 << R) / 4; q++) {
-            Real m[8];
-            load_matrix<Real>(t[q].m, m);
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                ip_cmul(a[4 * q + k].x, a[4 * q + k].y, m[2 * k], m[2 * k + 1], -m[2 * k + 1]);
-            }
+        for (int r = 0; r < (1 << R); r++) {
+            const uint32_t l = r ^ xr;
+            const A2 f = load_c<Real, A2>(z + (l >> 2) * (sizeof(DevOp<Real>) / sizeof(Real)) + 2 * (l & 3));
+            ip_cmul2(a[r], f);
         }
     }
     return 1 + nrec;
@@ -566,25 +594,41 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
 
 // Applies record `op` (and, for a layer, its matrix records); returns the
 // number of records consumed.
+//
+// Register relabeling: a thread keeps `xr`, and register r holds the
+// amplitude whose register label is r ^ xr.  An X on a register bit whose
+// controls (if any) lie on thread or non-tile bits -- most CNOTs of a pass --
+// only flips a bit of xr.  Gates on a register bit whose xr bit is set use
+// the bit-swapped matrix, register-bit control values are read through xr,
+// and the next transpose or the store puts every amplitude where its label
+// says (xr is then 0 again).
 template <typename Real, typename A2, int R>
 __device__ __forceinline__ int apply_op(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, uint64_t base,
-                                        uint32_t thr) {
+                                        uint32_t thr, uint32_t &xr) {
     const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));  // kind, tpos, cm_reg, cv_reg
     const int kind = (int)hdr.x, tpos = (int)hdr.y;
-    if (kind == K_PHASE_BLOCK) return apply_phase_block<Real, A2, R>(a, op, base, thr);
+    if (kind == K_PHASE_BLOCK) return apply_phase_block<Real, A2, R>(a, op, base, thr, xr);
     if (kind == K_LAYER || kind == K_LAYER_REAL) {
         const uint32_t mask = hdr.z;  // active register bits
-        if (kind == K_LAYER) LayerStep<Real, A2, R, 0, false>::run(a, op + 1, mask);
-        else LayerStep<Real, A2, R, 0, true>::run(a, op + 1, mask);
+        if (kind == K_LAYER) LayerStep<Real, A2, R, 0, false>::run(a, op + 1, mask, xr);
+        else LayerStep<Real, A2, R, 0, true>::run(a, op + 1, mask, xr);
         return 1 + __popc(mask);
     }
     const uint4 th = __ldg(reinterpret_cast<const uint4 *>(op) + 1);                 // cm_thr, cv_thr
     const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(op) + 2);       // cm_glob, cv_glob
     if ((base & gl.x) != gl.y) return 1;
     if ((thr & th.x) != th.y) return 1;
-    const uint32_t cm = hdr.z, cv = hdr.w;
+    const uint32_t cm = hdr.z, cv = hdr.w ^ (xr & hdr.z);
     if (tpos < R) {
-        RegTarget<Real, A2, R, 0>::run(1u << tpos, 1u << kind, a, op->m, cm, cv);
+        if (kind == K_SWAP && cm == 0) {
+            xr ^= 1u << tpos;
+            return 1;
+        }
+        // a phase gate seen through a swapped label is diag(d1, 1): run it as
+        // a diagonal gate on the bit-swapped matrix
+        const bool flip = (xr >> tpos) & 1u;
+        const int k = (kind == K_PHASE && flip) ? K_DIAG : kind;
+        RegTarget<Real, A2, R, 0>::run(1u << tpos, 1u << k, a, op->m, cm, cv, flip);
         return 1;
     }
     // diagonal gate on a thread bit or a non-tile index bit
@@ -602,11 +646,13 @@ __device__ __forceinline__ int apply_op(A2 (&a)[1 << R], const DevOp<Real> *__re
 
 template <typename Real, typename A2, int R, int W, int FROM, int TO>
 __device__ __forceinline__ void transpose_t(A2 (&a)[1 << R], A2 *sm, uint32_t lane, uint32_t warp,
-                                            bool sync_cta_before, bool cross) {
+                                            bool sync_cta_before, bool cross, uint32_t xr) {
     if (sync_cta_before) __syncthreads();
     else __syncwarp();
+    // register r holds label r ^ xr; the index and the swizzle are XOR-linear
+    const uint32_t xo = swz<Real, R>(local_index<R, W, FROM>(0, 0, xr));
 #pragma unroll
-    for (int r = 0; r < (1 << R); r++) sm[swz<Real, R>(local_index<R, W, FROM>(lane, warp, r))] = a[r];
+    for (int r = 0; r < (1 << R); r++) sm[swz<Real, R>(local_index<R, W, FROM>(lane, warp, r)) ^ xo] = a[r];
     if (cross) __syncthreads();
     else __syncwarp();
 #pragma unroll
@@ -615,27 +661,27 @@ __device__ __forceinline__ void transpose_t(A2 (&a)[1 << R], A2 *sm, uint32_t la
 
 template <typename Real, typename A2, int R, int W, int FROM>
 __device__ __forceinline__ void transpose_from(int to, A2 (&a)[1 << R], A2 *sm, uint32_t lane, uint32_t warp,
-                                               bool sync_cta_before, bool cross) {
+                                               bool sync_cta_before, bool cross, uint32_t xr) {
     switch (to) {
-        case LAYOUT_C: transpose_t<Real, A2, R, W, FROM, LAYOUT_C>(a, sm, lane, warp, sync_cta_before, cross); break;
-        case LAYOUT_B: transpose_t<Real, A2, R, W, FROM, LAYOUT_B>(a, sm, lane, warp, sync_cta_before, cross); break;
+        case LAYOUT_C: transpose_t<Real, A2, R, W, FROM, LAYOUT_C>(a, sm, lane, warp, sync_cta_before, cross, xr); break;
+        case LAYOUT_B: transpose_t<Real, A2, R, W, FROM, LAYOUT_B>(a, sm, lane, warp, sync_cta_before, cross, xr); break;
         case LAYOUT_E:
-            if (R == 4) transpose_t<Real, A2, R, W, FROM, LAYOUT_E>(a, sm, lane, warp, sync_cta_before, cross);
+            if (R == 4) transpose_t<Real, A2, R, W, FROM, LAYOUT_E>(a, sm, lane, warp, sync_cta_before, cross, xr);
             break;
-        default: transpose_t<Real, A2, R, W, FROM, LAYOUT_A>(a, sm, lane, warp, sync_cta_before, cross); break;
+        default: transpose_t<Real, A2, R, W, FROM, LAYOUT_A>(a, sm, lane, warp, sync_cta_before, cross, xr); break;
     }
 }
 
 template <typename Real, typename A2, int R, int W>
 __device__ __forceinline__ void transpose(int from, int to, A2 (&a)[1 << R], A2 *sm, uint32_t lane, uint32_t warp,
-                                          bool sync_cta_before, bool cross) {
+                                          bool sync_cta_before, bool cross, uint32_t xr) {
     switch (from) {
-        case LAYOUT_C: transpose_from<Real, A2, R, W, LAYOUT_C>(to, a, sm, lane, warp, sync_cta_before, cross); break;
-        case LAYOUT_B: transpose_from<Real, A2, R, W, LAYOUT_B>(to, a, sm, lane, warp, sync_cta_before, cross); break;
+        case LAYOUT_C: transpose_from<Real, A2, R, W, LAYOUT_C>(to, a, sm, lane, warp, sync_cta_before, cross, xr); break;
+        case LAYOUT_B: transpose_from<Real, A2, R, W, LAYOUT_B>(to, a, sm, lane, warp, sync_cta_before, cross, xr); break;
         case LAYOUT_E:
-            if (R == 4) transpose_from<Real, A2, R, W, LAYOUT_E>(to, a, sm, lane, warp, sync_cta_before, cross);
+            if (R == 4) transpose_from<Real, A2, R, W, LAYOUT_E>(to, a, sm, lane, warp, sync_cta_before, cross, xr);
             break;
-        default: transpose_from<Real, A2, R, W, LAYOUT_A>(to, a, sm, lane, warp, sync_cta_before, cross); break;
+        default: transpose_from<Real, A2, R, W, LAYOUT_A>(to, a, sm, lane, warp, sync_cta_before, cross, xr); break;
     }
 }
 
@@ -666,7 +712,7 @@ __device__ __forceinline__ void load_tile(typename V2<Real>::T (&a)[1 << R],
 template <typename Real, int R, int W, int LAY>
 __device__ __forceinline__ void store_tile(const typename V2<Real>::T (&a)[1 << R],
                                            typename V2<Real>::T *__restrict__ state, const PassArgs &pa,
-                                           uint64_t base, uint32_t warp) {
+                                           uint64_t base, uint32_t warp, uint32_t xr) {
     using A2 = typename V2<Real>::T;
     // The lane index is re-read so the store geometry is recomputed here
     // instead of being held in registers through every phase.
@@ -674,7 +720,11 @@ __device__ __forceinline__ void store_tile(const typename V2<Real>::T (&a)[1 << 
     asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
     uint64_t off, rs[R];
     thread_geometry<R, W, LAY>(pa, lane, warp, off, rs);
-    StoreF<A2, R> f{a, state + (base | off), rs};
+    uint64_t xo = 0;
+#pragma unroll
+    for (int q = 0; q < R; q++)
+        if ((xr >> q) & 1u) xo |= rs[q];
+    StoreF<A2, R> f{a, state, base | off | xo, rs};
     Unroll<1 << R>::run(f);
 }
 
@@ -702,22 +752,25 @@ __device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ stat
         }
     }
     bool prev_cross = false;
+    uint32_t xr = 0;  // register relabeling (apply_op)
     for (int p = pa.phase_begin; p < pa.phase_end; p++) {
         const DevPhase ph = pa.phases[p];
         if (ph.layout != cur) {
-            transpose<Real, A2, R, W>(cur, ph.layout, a, sm, lane, warp, prev_cross || ph.xwarp, ph.xwarp != 0);
+            transpose<Real, A2, R, W>(cur, ph.layout, a, sm, lane, warp, prev_cross || ph.xwarp, ph.xwarp != 0, xr);
+            xr = 0;
             prev_cross = ph.xwarp != 0;
             cur = ph.layout;
         }
-        for (int i = ph.op_begin; i < ph.op_end;) i += apply_op<Real, A2, R>(a, ops + i, base, thr);
+        for (int i = ph.op_begin; i < ph.op_end;) i += apply_op<Real, A2, R>(a, ops + i, base, thr, xr);
     }
     if (cur != pa.store_layout) {
         const bool cross = (cur == LAYOUT_A) != (pa.store_layout == LAYOUT_A);
-        transpose<Real, A2, R, W>(cur, pa.store_layout, a, sm, lane, warp, prev_cross || cross, cross);
+        transpose<Real, A2, R, W>(cur, pa.store_layout, a, sm, lane, warp, prev_cross || cross, cross, xr);
+        xr = 0;
         cur = pa.store_layout;
     }
-    if (cur == LAYOUT_A) store_tile<Real, R, W, LAYOUT_A>(a, state, pa, base, warp);
-    else store_tile<Real, R, W, LAYOUT_C>(a, state, pa, base, warp);
+    if (cur == LAYOUT_A) store_tile<Real, R, W, LAYOUT_A>(a, state, pa, base, warp, xr);
+    else store_tile<Real, R, W, LAYOUT_C>(a, state, pa, base, warp, xr);
     if (pa.flags & PASS_NORM) {
         double acc = 0.0;
 #pragma unroll
