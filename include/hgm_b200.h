@@ -217,6 +217,12 @@ void hgm_server_free(hgm_server *s);
  * state can never fit the budget. */
 int hgm_server_submit(hgm_server *s, const hgm_circuit *c, int qubits, int64_t init_index, uint64_t result_mask,
                       int64_t *id);
+/* Queues an already built plan (hgm_plan_create, the server's precision):
+ * the request's work is then all on the device.  The plan is uploaded here
+ * if it has not run yet.  It is borrowed: it must stay alive, and not run
+ * elsewhere, until this request's result has been polled (its
+ * renormalisation scratch belongs to the plan). */
+int hgm_server_submit_plan(hgm_server *s, const hgm_plan *p, int64_t init_index, uint64_t result_mask, int64_t *id);
 /* Moves up to `max` finished results into `out` (waiting up to wait_ms for
  * the first); *n = how many. */
 int hgm_server_poll(hgm_server *s, hgm_result *out, int max, int *n, int wait_ms);

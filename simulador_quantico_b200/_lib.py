@@ -96,6 +96,7 @@ def _load():
         "hgm_server_create": ([P(ServerOpts), P(vp)], i),
         "hgm_server_free": ([vp], None),
         "hgm_server_submit": ([vp, vp, i, i64, C.c_uint64, P(i64)], i),
+        "hgm_server_submit_plan": ([vp, vp, i64, C.c_uint64, P(i64)], i),
         "hgm_server_poll": ([vp, P(Result), i, P(i), i], i),
         "hgm_server_pending": ([vp, P(i), P(i), P(i64)], i),
         "hgm_server_result_state": ([vp, i64], vp),

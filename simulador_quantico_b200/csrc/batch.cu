@@ -196,7 +196,7 @@ namespace {
 
 template <typename Real, int R, int W>
 int batch_setup(Batch *b) {
-    const int smem = (1 << (5 + R + W)) * (int)sizeof(typename V2<Real>::T);
+    const int smem = tile_smem_elems<R, W>() * (int)sizeof(typename V2<Real>::T);
     cudaError_t e = cudaFuncSetAttribute(batch_kernel<Real, R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "batch kernel attribute: %s", cudaGetErrorString(e));
     int per_sm = 0, dev = 0, sms = 0;

@@ -129,7 +129,7 @@ template <typename Real, int R, int W>
 static int setup_pass_kernel() {
     static bool done = false;
     if (done) return HGM_OK;
-    const int smem = (1 << (5 + R + W)) * (int)sizeof(typename V2<Real>::T);
+    const int smem = tile_smem_elems<R, W>() * (int)sizeof(typename V2<Real>::T);
     cudaError_t e = cudaFuncSetAttribute(pass_kernel<Real, R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess && HGM_SMEM_CARVEOUT >= 0)
         e = cudaFuncSetAttribute(pass_kernel<Real, R, W>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -144,7 +144,7 @@ static int launch_pass(void *state, const PassArgs &pa, cudaStream_t st) {
     int rc = setup_pass_kernel<Real, R, W>();
     if (rc) return rc;
     const uint64_t tiles = 1ull << (pa.n - pa.k);
-    const int smem = (1 << (5 + R + W)) * (int)sizeof(typename V2<Real>::T);
+    const int smem = tile_smem_elems<R, W>() * (int)sizeof(typename V2<Real>::T);
     pass_kernel<Real, R, W><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<typename V2<Real>::T *>(state),
                                                                     pa);
     count_launch();
@@ -176,6 +176,11 @@ static int launch_small(State *s, const Plan *p, int iterations, cudaStream_t st
 int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
     if (s->qubits != p->qubits) return fail(HGM_ERR_INVALID, "plan is for %d qubits, state has %d", p->qubits, s->qubits);
     if (s->precision != p->precision) return fail(HGM_ERR_INVALID, "plan and state precision differ");
+    // every device pointer a launch passes must exist: an op list that was
+    // never uploaded is refused here, not read through a null pointer
+    if ((!p->ops_bytes.empty() && !p->d_ops) || (!p->phases.empty() && !p->d_phases) ||
+        (p->renorm_every > 0 && !p->small && !p->d_norm))
+        return fail(HGM_ERR_INVALID, "plan used before upload_plan");
     cudaStream_t st = pick(stream);
     if (!st) return HGM_ERR_CUDA;
     if (p->small) return p->n_small_ops ? (p->precision == HGM_F64 ? launch_small<double>(s, p, iterations, st)

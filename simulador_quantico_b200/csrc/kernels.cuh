@@ -74,10 +74,28 @@ struct V2<float> {
     using T = float2;
 };
 
-template <typename Real, int R>
-__device__ __forceinline__ uint32_t swz(uint32_t j) {
-    constexpr uint32_t S = sizeof(Real) == 8 ? 7u : 15u;
-    return j ^ ((j >> R) & S);
+// Shared-memory slot of local index j in a transpose: j + (j >> R).  The
+// padding keeps every layout's warp accesses free of bank conflicts (a lane
+// stride of 2^R elements becomes 2^R + 1) and, unlike an XOR swizzle, it is
+// additive over a layout's disjoint lane/warp and register bits, so the slot
+// of register r is the thread's base slot plus r times a constant.
+template <int R>
+__device__ __forceinline__ uint32_t pad_slot(uint32_t j) {
+    return j + (j >> R);
+}
+
+// Slot step between consecutive register labels of a layout: its register
+// bits start at local bit s, and pad_slot(l << s) = l * (2^s + 2^(s-R)).
+template <int R, int W, int LAY>
+__host__ __device__ constexpr uint32_t reg_slot_stride() {
+    constexpr int s = LAY == LAYOUT_C ? 5 : LAY == LAYOUT_B ? 0 : LAY == LAYOUT_E ? 4 : 5 + W;
+    return (1u << s) + (s >= R ? (1u << (s - R)) : 0u);
+}
+
+// Shared memory of one tile's transposes, in amplitudes.
+template <int R, int W>
+__host__ __device__ constexpr int tile_smem_elems() {
+    return (1 << (5 + R + W)) + (1 << (5 + W));
 }
 
 template <int R, int W, int LAY>
@@ -649,14 +667,21 @@ __device__ __forceinline__ void transpose_t(A2 (&a)[1 << R], A2 *sm, uint32_t la
                                             bool sync_cta_before, bool cross, uint32_t xr) {
     if (sync_cta_before) __syncthreads();
     else __syncwarp();
-    // register r holds label r ^ xr; the index and the swizzle are XOR-linear
-    const uint32_t xo = swz<Real, R>(local_index<R, W, FROM>(0, 0, xr));
+    // register r holds label r ^ xr
+    constexpr uint32_t sf = reg_slot_stride<R, W, FROM>(), st = reg_slot_stride<R, W, TO>();
+    A2 *w = sm + pad_slot<R>(local_index<R, W, FROM>(lane, warp, 0));
+    if (xr == 0) {
 #pragma unroll
-    for (int r = 0; r < (1 << R); r++) sm[swz<Real, R>(local_index<R, W, FROM>(lane, warp, r)) ^ xo] = a[r];
+        for (int r = 0; r < (1 << R); r++) w[sf * r] = a[r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) w[sf * (r ^ xr)] = a[r];
+    }
     if (cross) __syncthreads();
     else __syncwarp();
+    const A2 *rd = sm + pad_slot<R>(local_index<R, W, TO>(lane, warp, 0));
 #pragma unroll
-    for (int r = 0; r < (1 << R); r++) a[r] = sm[swz<Real, R>(local_index<R, W, TO>(lane, warp, r))];
+    for (int r = 0; r < (1 << R); r++) a[r] = rd[st * r];
 }
 
 template <typename Real, typename A2, int R, int W, int FROM>

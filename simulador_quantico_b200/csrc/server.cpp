@@ -1,7 +1,8 @@
 // Serving mode: continuous batching of circuits on one GPU.
 //
 // Clients submit circuits at any time (hgm_server_submit plans them on the
-// calling thread).  One worker thread
+// calling thread; hgm_server_submit_plan takes a plan built beforehand).  One
+// worker thread
 //   * admits queued requests in arrival order while a slot is free and the
 //     request's state bytes (16*2^n FP64, 8*2^n FP32) fit the HBM budget
 //     (a request larger than the whole budget is refused);
@@ -26,6 +27,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -45,7 +47,8 @@ struct Request {
     int n = 0;
     int64_t init_index = 0;
     uint64_t result_mask = 0;
-    std::unique_ptr<Plan> plan;
+    std::unique_ptr<Plan> owned;  // planned by hgm_server_submit
+    const Plan *plan = nullptr;   // owned, or borrowed (hgm_server_submit_plan)
     int64_t bytes = 0;
     double t_submit = 0, t_admit = 0, t_done = 0;
     State state;  // device state (pool memory)
@@ -81,6 +84,7 @@ struct Server {
     std::thread worker;
     int inflight = 0;
     int error = HGM_OK;
+    std::string error_msg;  // the worker's message for `error`, reported by hgm_server_poll
 
     ~Server() {
         stop = true;
@@ -151,7 +155,7 @@ struct Server {
         r->state.qubits = r->n;
         r->state.precision = opts.precision;
         int rc = launch_set_basis(&r->state, r->init_index, s.stream);
-        if (!rc) rc = launch_plan(&r->state, r->plan.get(), 1, s.stream);
+        if (!rc) rc = launch_plan(&r->state, r->plan, 1, s.stream);
         if (!rc) rc = launch_norm_async(&r->state, s.partials, s.dres, s.stream);
         if (!rc && r->result_mask) rc = launch_argmax_async(&r->state, r->result_mask, s.partials, s.ibest, s.dres + 2, s.stream);
         if (rc) return rc;
@@ -161,6 +165,16 @@ struct Server {
     }
 
     int device = 0;
+
+    void enqueue(Request *r, int64_t *id) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            r->id = next_id++;
+            if (id) *id = r->id;
+            queue.push_back(r);
+        }
+        cv.notify_all();
+    }
 
     void loop() {
         cudaSetDevice(device);
@@ -175,7 +189,12 @@ struct Server {
                     progress = true;
                 } else if (q != cudaErrorNotReady) {
                     s.req->status = HGM_ERR_CUDA;
-                    error = fail(HGM_ERR_CUDA, "request execution: %s", cudaGetErrorString(q));
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        error_msg = "request " + std::to_string(s.req->id) + " (" + std::to_string(s.req->n) +
+                                    " qubits) execution: " + cudaGetErrorString(q);
+                        error = HGM_ERR_CUDA;
+                    }
                     finish(s);
                     progress = true;
                 }
@@ -274,17 +293,37 @@ int hgm_server_submit(hgm_server *ss, const hgm_circuit *c, int qubits, int64_t 
     hgm_plan_opts o;
     hgm_plan_default_opts(&o, s->opts.precision);
     o.warp_bits = s->opts.warp_bits;
-    r->plan.reset(new Plan());
-    int rc = build_plan(reinterpret_cast<const Circuit *>(c)->ops, qubits, o, r->plan.get());
-    if (!rc) rc = upload_plan(r->plan.get());
+    r->owned.reset(new Plan());
+    int rc = build_plan(reinterpret_cast<const Circuit *>(c)->ops, qubits, o, r->owned.get());
+    if (!rc) rc = upload_plan(r->owned.get());
     if (rc) return rc;
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        r->id = s->next_id++;
-        if (id) *id = r->id;
-        s->queue.push_back(r.release());
-    }
-    s->cv.notify_all();
+    r->plan = r->owned.get();
+    s->enqueue(r.release(), id);
+    return HGM_OK;
+}
+
+int hgm_server_submit_plan(hgm_server *ss, const hgm_plan *pp, int64_t init_index, uint64_t result_mask,
+                           int64_t *id) {
+    Server *s = reinterpret_cast<Server *>(ss);
+    const Plan *p = reinterpret_cast<const Plan *>(pp);
+    if (!s || !p) return fail(HGM_ERR_INVALID, "null argument");
+    if (p->precision != s->opts.precision) return fail(HGM_ERR_INVALID, "plan precision differs from the server's");
+    const int qubits = p->qubits;
+    if (init_index < 0 || init_index >= (int64_t(1) << qubits)) return fail(HGM_ERR_INVALID, "initial index outside state");
+    std::unique_ptr<Request> r(new Request());
+    r->t_submit = now_s();
+    r->n = qubits;
+    r->init_index = init_index;
+    r->result_mask = result_mask;
+    r->bytes = (int64_t(1) << qubits) * (s->opts.precision == HGM_F64 ? 16 : 8);
+    if (r->bytes > s->opts.budget_bytes)
+        return fail(HGM_ERR_BUSY, "state of %lld bytes exceeds the %lld-byte budget", (long long)r->bytes,
+                    (long long)s->opts.budget_bytes);
+    // a plan is uploaded on first use; do it here, on the calling thread
+    const int rc = upload_plan(const_cast<Plan *>(p));
+    if (rc) return rc;
+    r->plan = p;
+    s->enqueue(r.release(), id);
     return HGM_OK;
 }
 
@@ -300,7 +339,8 @@ int hgm_server_poll(hgm_server *ss, hgm_result *out, int max, int *n, int wait_m
         s->results.pop_front();
     }
     *n = k;
-    return s->error;
+    if (s->error) return fail(s->error, "%s", s->error_msg.c_str());
+    return HGM_OK;
 }
 
 int hgm_server_pending(hgm_server *ss, int *queued, int *inflight, int64_t *bytes_in_use) {

@@ -119,9 +119,14 @@ class Plan:
         v = [C.c_int64() for _ in range(4)]
         check(lib.hgm_plan_stats(self.h, *[C.byref(x) for x in v]))
         wb, small = C.c_int(), C.c_int()
-        check(lib.hgm_plan_export(self.h, None, None, None, None, None, None, C.byref(wb), C.byref(small)))
+        nph, nb = C.c_int64(), C.c_int64()
+        check(lib.hgm_plan_export(self.h, None, None, None, C.byref(nph), None, C.byref(nb), C.byref(wb),
+                                  C.byref(small)))
+        # bytes copied to the device when the plan is created: op records and phase table
+        upload = nb.value + 16 * nph.value
         return dict(ops=v[0].value, passes=v[1].value, phases=v[2].value, transposes=v[3].value,
-                    warp_bits=wb.value, reg_bits=4 if self.precision == HGM_F64 else 5, small=bool(small.value))
+                    warp_bits=wb.value, reg_bits=4 if self.precision == HGM_F64 else 5, small=bool(small.value),
+                    upload_bytes=upload)
 
 
 class State:
@@ -277,6 +282,14 @@ class Server:
         rid = C.c_int64()
         check(lib.hgm_server_submit(self.h, circuit.h, qubits, init_index, result_mask, C.byref(rid)))
         self.qubits[rid.value] = qubits
+        return rid.value
+
+    def submit_plan(self, plan: "Plan", init_index: int = 0, result_mask: int = 0) -> int:
+        """Queues an already built (device-resident) plan; the plan must stay
+        alive, and not run elsewhere, until this request's result is polled."""
+        rid = C.c_int64()
+        check(lib.hgm_server_submit_plan(self.h, plan.h, init_index, result_mask, C.byref(rid)))
+        self.qubits[rid.value] = plan.qubits
         return rid.value
 
     def poll(self, max_results=256, wait_ms=0):

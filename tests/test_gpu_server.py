@@ -99,3 +99,29 @@ def test_fp64_server_matches_oracle(sq):
         assert np.abs(got - oracle_state(spec, "f64")).max() < 1e-12
         srv.release(r["id"])
     srv.close()
+
+
+def test_submit_plan_matches_submit(sq):
+    """A request queued as a prebuilt plan (hgm_server_submit_plan) gives the
+    same result as the same circuit submitted for the server to plan; a plan
+    of the wrong precision is refused."""
+    reqs = request_mix(23, 12)
+    srv = sq.Server("f32", budget_bytes=1 << 30, max_inflight=4, keep_states=True)
+    plans, ids = [], {}
+    for spec, mask in reqs:
+        c = spec.build(sq.Circuit())
+        p = sq.Plan(c, spec.qubits, "f32")
+        plans.append(p)
+        ids[srv.submit_plan(p, spec.init_index, mask)] = ("plan", spec)
+        ids[srv.submit(c, spec.qubits, spec.init_index, mask)] = ("circuit", spec)
+    results = {r["id"]: r for r in srv.drain(2 * len(reqs))}
+    assert all(r["status"] == 0 for r in results.values())
+    rids = sorted(ids)
+    for a, b in zip(rids[0::2], rids[1::2]):
+        assert ids[a][0] == "plan" and ids[b][0] == "circuit"
+        ga, gb = srv.result_state(a).download(), srv.result_state(b).download()
+        assert np.array_equal(ga, gb), ids[a][1].name
+        assert results[a]["argmax"] == results[b]["argmax"]
+    with pytest.raises(sq.HgmError):
+        srv.submit_plan(sq.Plan(reqs[0][0].build(sq.Circuit()), reqs[0][0].qubits, "f64"))
+    srv.close()
