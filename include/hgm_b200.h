@@ -213,8 +213,9 @@ typedef struct hgm_result {
 void hgm_server_default_opts(hgm_server_opts *o, int precision);
 int hgm_server_create(const hgm_server_opts *opts, hgm_server **out);
 void hgm_server_free(hgm_server *s);
-/* Plans the circuit on the calling thread and queues it. HGM_ERR_BUSY if its
- * state can never fit the budget. */
+/* Copies the circuit and queues it; planner threads plan and upload it while
+ * earlier requests run (a planning failure comes back as the result's
+ * status).  HGM_ERR_BUSY if its state can never fit the budget. */
 int hgm_server_submit(hgm_server *s, const hgm_circuit *c, int qubits, int64_t init_index, uint64_t result_mask,
                       int64_t *id);
 /* Queues an already built plan (hgm_plan_create, the server's precision):

@@ -1,11 +1,12 @@
 // Serving mode: continuous batching of circuits on one GPU.
 //
-// Clients submit circuits at any time (hgm_server_submit plans them on the
-// calling thread; hgm_server_submit_plan takes a plan built beforehand).  One
-// worker thread
-//   * admits queued requests in arrival order while a slot is free and the
-//     request's state bytes (16*2^n FP64, 8*2^n FP32) fit the HBM budget
-//     (a request larger than the whole budget is refused);
+// Clients submit circuits at any time.  hgm_server_submit copies the circuit
+// and returns; a few planner threads plan and upload submitted circuits while
+// earlier requests run (hgm_server_submit_plan takes a plan built
+// beforehand).  One worker thread
+//   * admits planned requests in the order their plans are ready, while a
+//     slot is free and the request's state bytes (16*2^n FP64, 8*2^n FP32)
+//     fit the HBM budget (a request larger than the whole budget is refused);
 //   * gives each admitted request a slot -- a CUDA stream with its own
 //     reduction scratch -- allocates the state stream-ordered
 //     (cudaMallocAsync from the device's memory pool, so no allocation
@@ -20,6 +21,7 @@
 // and fixed-order reductions.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -47,7 +49,9 @@ struct Request {
     int n = 0;
     int64_t init_index = 0;
     uint64_t result_mask = 0;
-    std::unique_ptr<Plan> owned;  // planned by hgm_server_submit
+    std::vector<Op> ops;          // hgm_server_submit: the circuit, until a planner thread plans it
+    hgm_plan_opts popts{};
+    std::unique_ptr<Plan> owned;  // planned by a planner thread
     const Plan *plan = nullptr;   // owned, or borrowed (hgm_server_submit_plan)
     int64_t bytes = 0;
     double t_submit = 0, t_admit = 0, t_done = 0;
@@ -82,14 +86,22 @@ struct Server {
     int64_t next_id = 1;
     std::atomic<bool> stop{false};
     std::thread worker;
+    std::deque<Request *> to_plan;   // submitted circuits waiting for a planner thread
+    std::condition_variable plan_cv;
+    std::vector<std::thread> planners;
+    int planning = 0;                // circuits being planned
     int inflight = 0;
     int error = HGM_OK;
     std::string error_msg;  // the worker's message for `error`, reported by hgm_server_poll
 
     ~Server() {
         stop = true;
+        plan_cv.notify_all();
         cv.notify_all();
+        for (std::thread &t : planners)
+            if (t.joinable()) t.join();
         if (worker.joinable()) worker.join();
+        for (Request *r : to_plan) delete r;
         for (Slot &s : slots) {
             if (s.stream) cudaStreamSynchronize(s.stream);
             if (s.req) {
@@ -165,6 +177,45 @@ struct Server {
     }
 
     int device = 0;
+
+    // Planner thread: plans and uploads submitted circuits, then hands them to
+    // the worker.  A request is admitted once its plan is ready, so a quick
+    // circuit is not held behind a slow one.
+    void plan_loop() {
+        cudaSetDevice(device);
+        for (;;) {
+            Request *r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                plan_cv.wait(lk, [this] { return stop || !to_plan.empty(); });
+                if (stop) return;
+                r = to_plan.front();
+                to_plan.pop_front();
+                planning++;
+            }
+            r->owned.reset(new Plan());
+            int rc = build_plan(r->ops, r->n, r->popts, r->owned.get());
+            if (!rc) rc = upload_plan(r->owned.get());
+            std::vector<Op>().swap(r->ops);
+            r->plan = r->owned.get();
+            std::lock_guard<std::mutex> lk(mu);
+            planning--;
+            if (rc) {  // never runs: its result carries the planning status
+                hgm_result res{};
+                res.id = r->id;
+                res.status = rc;
+                res.qubits = r->n;
+                res.latency_s = now_s() - r->t_submit;
+                res.argmax = -1;
+                results.push_back(res);
+                delete r;
+                results_cv.notify_all();
+            } else {
+                queue.push_back(r);
+                cv.notify_all();
+            }
+        }
+    }
 
     void enqueue(Request *r, int64_t *id) {
         {
@@ -270,6 +321,9 @@ int hgm_server_create(const hgm_server_opts *opts, hgm_server **out) {
     cudaGetDevice(&s->device);
     Server *raw = s.get();
     s->worker = std::thread([raw] { raw->loop(); });
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int np = (int)std::max(1u, std::min(8u, hw / 2));
+    for (int i = 0; i < np; i++) s->planners.emplace_back([raw] { raw->plan_loop(); });
     *out = reinterpret_cast<hgm_server *>(s.release());
     return HGM_OK;
 }
@@ -290,15 +344,16 @@ int hgm_server_submit(hgm_server *ss, const hgm_circuit *c, int qubits, int64_t 
     if (r->bytes > s->opts.budget_bytes)
         return fail(HGM_ERR_BUSY, "state of %lld bytes exceeds the %lld-byte budget", (long long)r->bytes,
                     (long long)s->opts.budget_bytes);
-    hgm_plan_opts o;
-    hgm_plan_default_opts(&o, s->opts.precision);
-    o.warp_bits = s->opts.warp_bits;
-    r->owned.reset(new Plan());
-    int rc = build_plan(reinterpret_cast<const Circuit *>(c)->ops, qubits, o, r->owned.get());
-    if (!rc) rc = upload_plan(r->owned.get());
-    if (rc) return rc;
-    r->plan = r->owned.get();
-    s->enqueue(r.release(), id);
+    hgm_plan_default_opts(&r->popts, s->opts.precision);
+    r->popts.warp_bits = s->opts.warp_bits;
+    r->ops = reinterpret_cast<const Circuit *>(c)->ops;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        if (id) *id = r->id;
+        s->to_plan.push_back(r.release());
+    }
+    s->plan_cv.notify_one();
     return HGM_OK;
 }
 
@@ -347,7 +402,7 @@ int hgm_server_pending(hgm_server *ss, int *queued, int *inflight, int64_t *byte
     Server *s = reinterpret_cast<Server *>(ss);
     if (!s) return fail(HGM_ERR_INVALID, "null server");
     std::lock_guard<std::mutex> lk(s->mu);
-    if (queued) *queued = (int)s->queue.size();
+    if (queued) *queued = (int)(s->to_plan.size() + s->planning + s->queue.size());
     if (inflight) *inflight = s->inflight;
     if (bytes_in_use) *bytes_in_use = s->bytes_in_use;
     return HGM_OK;
