@@ -384,10 +384,12 @@ template <typename Real, typename A2, int R, int T>
 struct RegTarget {
     __device__ __forceinline__ static void run(uint32_t tbit, uint32_t kbit, A2 (&a)[1 << R],
                                                const Real *__restrict__ mp, uint32_t cm, uint32_t cv, bool flip) {
-        if (tbit & (1u << T)) {
-            if (cm == 0) reg_kind_c<Real, A2, R, T, false>(kbit, a, mp, cm, cv, flip);
-            else reg_kind_c<Real, A2, R, T, true>(kbit, a, mp, cm, cv, flip);
-        }
+        // one instantiation, with the per-pair control test: gates without
+        // register controls (cm = 0, every pair passes) are rare here, since
+        // uncontrolled dense gates go out as layers and uncontrolled X gates
+        // relabel, and a second copy of every body cost instruction-cache
+        // misses
+        if (tbit & (1u << T)) reg_kind_c<Real, A2, R, T, true>(kbit, a, mp, cm, cv, flip);
         RegTarget<Real, A2, R, T + 1>::run(tbit, kbit, a, mp, cm, cv, flip);
     }
 };
@@ -610,8 +612,16 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
     return 1 + nrec;
 }
 
-// Applies record `op` (and, for a layer, its matrix records); returns the
-// number of records consumed.
+// Records taken by the op whose head record is `hdr`: a phase block's terms
+// and table, a layer's matrices, or the record alone.
+__device__ __forceinline__ int op_records(const uint4 &hdr) {
+    if ((int)hdr.x == K_PHASE_BLOCK) return 1 + (int)hdr.y;
+    if ((int)hdr.x == K_LAYER || (int)hdr.x == K_LAYER_REAL) return 1 + __popc(hdr.z);
+    return 1;
+}
+
+// Applies record `op` (and, for a layer or phase block, the records that
+// follow it); its head record `hdr` is already loaded.
 //
 // Register relabeling: a thread keeps `xr`, and register r holds the
 // amplitude whose register label is r ^ xr.  An X on a register bit whose
@@ -621,43 +631,44 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
 // and the next transpose or the store puts every amplitude where its label
 // says (xr is then 0 again).
 template <typename Real, typename A2, int R>
-__device__ __forceinline__ int apply_op(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, uint64_t base,
-                                        uint32_t thr, uint32_t &xr) {
-    const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));  // kind, tpos, cm_reg, cv_reg
-    const int kind = (int)hdr.x, tpos = (int)hdr.y;
-    if (kind == K_PHASE_BLOCK) return apply_phase_block<Real, A2, R>(a, op, base, thr, xr);
+__device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, const uint4 hdr,
+                                         uint64_t base, uint32_t thr, uint32_t &xr) {
+    const int kind = (int)hdr.x, tpos = (int)hdr.y;  // hdr: kind, tpos, cm_reg, cv_reg of `op`
+    if (kind == K_PHASE_BLOCK) {
+        apply_phase_block<Real, A2, R>(a, op, base, thr, xr);
+        return;
+    }
     if (kind == K_LAYER || kind == K_LAYER_REAL) {
         const uint32_t mask = hdr.z;  // active register bits
         if (kind == K_LAYER) LayerStep<Real, A2, R, 0, false>::run(a, op + 1, mask, xr);
         else LayerStep<Real, A2, R, 0, true>::run(a, op + 1, mask, xr);
-        return 1 + __popc(mask);
+        return;
     }
     const uint4 th = __ldg(reinterpret_cast<const uint4 *>(op) + 1);                 // cm_thr, cv_thr
     const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(op) + 2);       // cm_glob, cv_glob
-    if ((base & gl.x) != gl.y) return 1;
-    if ((thr & th.x) != th.y) return 1;
+    if ((base & gl.x) != gl.y) return;
+    if ((thr & th.x) != th.y) return;
     const uint32_t cm = hdr.z, cv = hdr.w ^ (xr & hdr.z);
     if (tpos < R) {
         if (kind == K_SWAP && cm == 0) {
             xr ^= 1u << tpos;
-            return 1;
+            return;
         }
         // a phase gate seen through a swapped label is diag(d1, 1): run it as
         // a diagonal gate on the bit-swapped matrix
         const bool flip = (xr >> tpos) & 1u;
         const int k = (kind == K_PHASE && flip) ? K_DIAG : kind;
         RegTarget<Real, A2, R, 0>::run(1u << tpos, 1u << k, a, op->m, cm, cv, flip);
-        return 1;
+        return;
     }
     // diagonal gate on a thread bit or a non-tile index bit
     const int bv = tpos >= TPOS_GLOBAL ? (int)((base >> (tpos - TPOS_GLOBAL)) & 1)
                                        : (int)((thr >> (tpos - TPOS_THREAD)) & 1);
-    if (kind == K_PHASE && !bv) return 1;
+    if (kind == K_PHASE && !bv) return;
     const A2 f = load_c<Real, A2>(op->m + (bv ? 6 : 0));
     const Real fr = f.x, fi = f.y;
-    if (cm == 0) reg_scale<Real, A2, R, false>(a, fr, fi, cm, cv);
-    else reg_scale<Real, A2, R, true>(a, fr, fi, cm, cv);
-    return 1;
+    reg_scale<Real, A2, R, true>(a, fr, fi, cm, cv);
+    return;
 }
 
 // ---- layout transposes through shared memory --------------------------------
@@ -786,7 +797,13 @@ __device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ stat
             prev_cross = ph.xwarp != 0;
             cur = ph.layout;
         }
-        for (int i = ph.op_begin; i < ph.op_end;) i += apply_op<Real, A2, R>(a, ops + i, base, thr, xr);
+        // (loading the next op's head record while this op runs costs more
+        // in registers than it saves in load latency)
+        for (int i = ph.op_begin; i < ph.op_end;) {
+            const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(ops + i));
+            apply_op<Real, A2, R>(a, ops + i, hdr, base, thr, xr);
+            i += op_records(hdr);
+        }
     }
     if (cur != pa.store_layout) {
         const bool cross = (cur == LAYOUT_A) != (pa.store_layout == LAYOUT_A);
