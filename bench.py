@@ -8,8 +8,10 @@ Workloads (synthetic, seeded; see DESIGN.md for the shapes):
            server in FP32 with FP64 norm checks; metric served circuits/s
   layered  a 30-qubit, 40-layer random Rz/Ry + CNOT circuit in FP64; metric
            gate-layers/s (one step = the whole circuit)
-  grover   Grover search as grover.out runs it (27 qubits incl. the ancilla,
-           FP64); metric Grover iterations/s (one step = 64 iterations)
+  grover   Grover search, 26 qubits FP64, marked index 42 (the phase
+           oracle + diffusion form, no ancilla); metric Grover iterations/s
+           (one step = 64 iterations); the full 6433-iteration search is run
+           after the timed steps and its argmax checked
 
 Timing: W untimed warm-up steps, then K steps between a barrier and a device
 synchronize on both sides, timed with CUDA events on the library stream;
@@ -279,6 +281,129 @@ def cpu_baseline_layered(args, kind="reference"):
 
 
 # ---------------------------------------------------------------------------
+# Grover search (config 2): 26 qubits FP64, marked index 42
+# ---------------------------------------------------------------------------
+
+GROVER_N, GROVER_MARK, GROVER_STEP_ITERS = 26, 42, 64
+
+
+def grover_parts(sq, n, mark):
+    """The Grover circuit as two plans: H on every qubit, and one iteration
+    (phase oracle on |mark>, H^n, sign flip on |0..0>, H^n)."""
+    from simulador_quantico_b200 import workloads as wl
+
+    spec = wl.grover_search(n, mark)
+    (h_steps, _, _), (it_steps, _, _) = spec.calls
+    init, one = sq.Circuit(), sq.Circuit()
+    for c in (init, one):
+        for name, m in spec.gates.items():
+            c.add_gate(name, np.asarray(m, dtype=np.complex128))
+    init.set_function(h_steps, 1, True)
+    one.set_function(it_steps, 1, False)
+    return spec, init, one
+
+
+def workload_grover(args, dist, sq):
+    n, mark = args.qubits or GROVER_N, GROVER_MARK
+    spec, c_init, c_one = grover_parts(sq, n, mark)
+    total_iters = spec.meta["iterations"]
+    p_init, p_one = sq.Plan(c_init, n, "f64"), sq.Plan(c_one, n, "f64")
+    st = sq.State(n, "f64").set_basis(0).execute(p_init)
+    step_iters = GROVER_STEP_ITERS
+
+    def step():
+        st.execute(p_one, step_iters)
+
+    with ClockSampler(dist.local_rank) as clk:
+        ms, launches = run_timed(dist, sq, step, args.steps, args.warmup)
+    ms_step = dist.max(ms / args.steps)
+    value = dist.world * step_iters / (ms_step * 1e-3)
+    stats = p_one.stats()
+    S = st.nbytes
+    passes_per_step = stats["passes"] * step_iters
+    achieved = passes_per_step * 2 * S / (ms_step * 1e-3) / 1e9
+    # outside the timed region: finish the search and check the answer
+    done = (args.warmup + args.steps) * step_iters
+    st.set_basis(0).execute(p_init).execute(p_one, total_iters)
+    found, pmax = st.marginal_argmax((1 << n) - 1)
+    st.free()
+    peak, peak_kind = hbm_peak()
+    line = base_line(args, dist, "Grover iterations/s (26q FP64, marked index 42)", value, "iterations/s", ms_step,
+                     "f64", {"workload": f"grover-{n}q-fp64", "qubits": n, "marked": mark,
+                             "iterations_per_step": step_iters, "passes_per_iteration": stats["passes"],
+                             "state_bytes": S, "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"})
+    line["search"] = {"iterations": total_iters, "argmax": int(found), "probability": round(pmax, 12),
+                      "ok": bool(found == mark and pmax > 0.99), "timed_iterations_before_check": done}
+    line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4),
+                        "traffic": round(TRAFFIC_OVER_ALGO["f64"] * 2 * S / 1e9, 3), "traffic_unit": "GB per launch",
+                        "traffic_source": "ncu capture of the 26-qubit FP64 layered case (same state size)",
+                        "peak_source": peak_kind,
+                        "kernel": "pass_kernel<double,%d,%d>" % (stats["reg_bits"], stats["warp_bits"]),
+                        "algorithmic_bytes_per_launch": 2 * S}
+    line["gpu_launches"] = launches
+    line["clocks"] = clk.summary()
+    line["e2e"] = e2e_grover(dist, sq, c_init, c_one, n, step_iters) if not args.skip_e2e else None
+    if dist.rank == 0 and not args.skip_cpu:
+        line["cpu_baseline"] = cpu_baseline_grover(args, n, mark)
+    return line
+
+
+def e2e_grover(dist, sq, c_init, c_one, n, iters):
+    """One step through the reference's C-ABI: GpuExecutionWrapper with the PT list of one iteration and
+    iterations = 64, on a host state (1 GiB each way)."""
+    L = sq.load_dropin("f64")
+    L.setDevice(dist.local_rank)
+    host = np.zeros(1 << n, dtype=np.complex128)
+    host[0] = 1.0
+    L.GpuExecutionWrapper(host.ctypes.data, c_init.ref_pts("f64"), n, 4, 8, 1, 64, 2, 1)
+    pts = c_one.ref_pts("f64")
+    t0 = time.perf_counter()
+    L.GpuExecutionWrapper(host.ctypes.data, pts, n, 4, 8, 1, 64, 2, iters)
+    dt = dist.max(time.perf_counter() - t0)
+    return {"value": round(dist.world * iters / dt, 4), "unit": "iterations/s", "h2d_bytes_per_step": int(host.nbytes),
+            "d2h_bytes_per_step": int(host.nbytes), "path": "GpuExecutionWrapper (reference C-ABI), host state",
+            "seconds": round(dt, 3)}
+
+
+def cpu_baseline_grover(args, n, mark, n_s=22, iters=8):
+    """t_PAR_CPU on a bounded sample: 8 iterations at 22 qubits, scaled by 2^(n-22)."""
+    from oracle import cpu
+    from simulador_quantico_b200 import workloads as wl
+
+    threads = os.cpu_count() or 1
+    spec = wl.grover_search(n_s, mark, iterations=iters)
+    if cpu.ref_available("f64"):
+        r = cpu.RefDGM(n_s, "f64")
+        for name, m in spec.gates.items():
+            r.add_gate(name, m)
+        r.set_memory_value(0)
+        (h_steps, _, _), (it_steps, _, _) = spec.calls
+        r.set_function(h_steps, 1, True)
+        r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
+        r.execute(1)
+        r.set_function(it_steps, iters, False)
+        t0 = time.perf_counter()
+        r.execute(1)
+        dt = time.perf_counter() - t0
+        r.close()
+        kind = "reference"
+    else:
+        from oracle import circuit_lang as cl
+
+        ops = spec.build(cl.Circuit()).as_arrays()
+        s0 = cpu.basis_state(n_s, 0)
+        t0 = time.perf_counter()
+        cpu.run_regions(s0, n_s, ops, threads=threads)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    per_iter = dt / iters * (1 << (n - n_s))
+    return {"value": round(1.0 / per_iter, 6), "unit": "iterations/s", "cores": threads, "kind": kind,
+            "sample": f"{iters} Grover iterations at {n_s} qubits FP64 t_PAR_CPU ({dt:.2f} s), scaled "
+                      f"x{1 << (n - n_s)} to {n} qubits"}
+
+
+# ---------------------------------------------------------------------------
 # served stream (continuous batching)
 # ---------------------------------------------------------------------------
 
@@ -519,7 +644,7 @@ def cpu_baseline_served(args, reqs, n_cap=20, op_cap=400):
             "sample": f"{len(reqs)} requests of the served mix on t_PAR_CPU FP32; each run on <= {n_cap} qubits "
                       f"and its first <= {op_cap} gates, time scaled by state size and gate count"}
 
-WORKLOADS = {"layered": workload_layered, "served": workload_served}
+WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": workload_grover}
 
 
 def base_line(args, dist, metric, value, unit, ms_step, dtype, config):
@@ -533,6 +658,7 @@ def reference_arm(args, dist):
     if dist.rank != 0:
         return None
     fn = {"layered": cpu_baseline_layered,
+          "grover": lambda a: cpu_baseline_grover(a, a.qubits or GROVER_N, GROVER_MARK),
           "served": lambda a: cpu_baseline_served(a, served_requests(1000 + a.warmup, a.requests or 48))}.get(args.workload)
     if fn is None:
         return {"impl": "reference", "unavailable": f"no reference timing for workload {args.workload}"}
@@ -569,6 +695,7 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")
     args = ap.parse_args()
     args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
+                        "grover": "Grover iterations/s (26q FP64, marked index 42)",
                         "served": SERVED_METRIC}.get(args.workload, args.workload)
     dist = Dist()
     try:
