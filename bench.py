@@ -6,6 +6,9 @@ Workloads (synthetic, seeded; see DESIGN.md for the shapes):
   served   the serving stream: a seeded request mix (random layered
            circuits, QFTs, Grover searches) served by the continuous-batching
            server in FP32 with FP64 norm checks; metric served circuits/s
+  batched  512 circuits of 10-22 qubits (half QFTs, half random layered) in
+           one persistent kernel replayed from a CUDA graph, FP32 (value) and
+           FP64, autotuned; metric batched circuits/s
   layered  a 30-qubit, 40-layer random Rz/Ry + CNOT circuit in FP64; metric
            gate-layers/s (one step = the whole circuit)
   grover   Grover search, 26 qubits FP64, marked index 42 (the phase
@@ -404,6 +407,151 @@ def cpu_baseline_grover(args, n, mark, n_s=22, iters=8):
 
 
 # ---------------------------------------------------------------------------
+# batched launch (config 4): 512 circuits of 10-22 qubits in one graph
+# ---------------------------------------------------------------------------
+
+def batched_specs(seed, count=512, lo=10, hi=22):
+    """Half exact QFTs of random basis inputs, half 10-layer random Rz/Ry+CNOT circuits; qubits uniform."""
+    from simulador_quantico_b200 import workloads as wl
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        n = int(rng.integers(lo, hi + 1))
+        if i % 2:
+            specs.append(wl.qft(n, int(rng.integers(1 << n))))
+        else:
+            specs.append(wl.random_layered(n, 10, seed=seed * 10007 + i))
+    return specs
+
+
+def batched_one(args, dist, sq, specs, circuits, prec):
+    b = sq.Batch(prec, 2)
+    for spec, c in zip(specs, circuits):
+        b.add(c, spec.qubits, spec.init_index)
+    t0 = time.perf_counter()
+    tune = b.autotune()
+    tune_s = time.perf_counter() - t0
+    size = b.size()
+    inputs = sq.PinnedArray((len(specs),), np.int64)
+    inputs.array[:] = [spec.init_index for spec in specs]
+    b.set_inputs(inputs.array)
+
+    def step():
+        b.run()
+
+    ms, launches = run_timed(dist, sq, step, args.steps, args.warmup)
+    b.check()
+    ms_step = dist.max(ms / args.steps)
+    value = dist.world * len(specs) / (ms_step * 1e-3)
+    peak, peak_kind = hbm_peak()
+    achieved = size["pass_bytes"] / (ms_step * 1e-3) / 1e9
+    out = {"value": round(value, 4), "unit": "circuits/s", "ms_per_step": round(ms_step, 4),
+           "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                        "kernel": f"batch_kernel ({prec})", "algorithmic_bytes_per_launch": size["pass_bytes"]},
+           "autotune": {**tune, "seconds": round(tune_s, 2)}, "tasks": size["tasks"], "tile_items": size["items"],
+           "arena_bytes": size["arena_bytes"], "gpu_launches": launches}
+    if not args.skip_e2e:
+        # end to end: the step's initial basis indices from pinned host memory, the graph, and every final
+        # state back into pinned host memory
+        host = sq.PinnedArray((size["arena_bytes"],), np.uint8)
+        for _ in range(2):
+            b.set_inputs(inputs.array).run().download(host)
+        sq.synchronize()
+        dist.barrier()
+        with sq.Timer() as t:
+            for _ in range(args.steps):
+                b.set_inputs(inputs.array).run().download(host)
+        sq.synchronize()
+        e_ms = dist.max(t.ms / args.steps)
+        out["e2e"] = {"value": round(dist.world * len(specs) / (e_ms * 1e-3), 4), "unit": "circuits/s",
+                      "h2d_bytes_per_step": int(inputs.nbytes), "d2h_bytes_per_step": int(size["arena_bytes"]),
+                      "path": "hgm_batch_set_inputs (pinned) -> hgm_batch_run -> hgm_batch_download (pinned)"}
+        del host
+    del b
+    return out
+
+
+def plain_batched(sq, specs, circuits, prec, limit_s):
+    """The same circuits one by one through the plain t_GPU drop-in (host state each), up to limit_s seconds."""
+    L = sq.load_dropin(prec)
+    L.setDevice(0)
+    dt = np.complex128 if prec == "f64" else np.complex64
+    done, t0 = 0, time.perf_counter()
+    for spec, c in zip(specs, circuits):
+        host = np.zeros(1 << spec.qubits, dtype=dt)
+        host[spec.init_index] = 1.0
+        L.GpuExecutionWrapper(host.ctypes.data, c.ref_pts(prec), spec.qubits, 4, 8, 1, 64, 2, 1)
+        done += 1
+        if time.perf_counter() - t0 > limit_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": round(done / el, 4), "unit": "circuits/s", "circuits": done, "seconds": round(el, 3),
+            "path": f"GpuExecutionWrapper {prec.upper()} (reference C-ABI), host state per circuit"}
+
+
+def workload_batched(args, dist, sq):
+    count = args.requests or 512
+    specs = batched_specs(4242, count)
+    circuits = [spec.build(sq.Circuit()) for spec in specs]
+    with ClockSampler(dist.local_rank) as clk:
+        f32 = batched_one(args, dist, sq, specs, circuits, "f32")
+    f64 = batched_one(args, dist, sq, specs, circuits, "f64")
+    line = base_line(args, dist, "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
+                     f32["value"], "circuits/s", f32["ms_per_step"], "f32",
+                     {"workload": f"batched-{count}", "circuits": count, "qubits": "uniform 10-22",
+                      "mix": "half QFT of a random basis input, half 10-layer random Rz/Ry+CNOT",
+                      "inputs": "plans and basis indices uploaded before the timed region; a step is one graph "
+                                "replay (state init + every circuit)",
+                      "l2": "arena of all states (~2.6 GB FP32) > 126 MB L2, no flush needed"})
+    line["gpu_launches"] = f32["gpu_launches"]
+    line["roofline"] = f32["roofline"]
+    line["fp32"] = f32
+    line["fp64"] = f64
+    line["e2e"] = f32.get("e2e")
+    line["clocks"] = clk.summary()
+    if not args.skip_e2e:
+        line["plain_fp32"] = plain_batched(sq, specs, circuits, "f32", args.plain_limit)
+        line["plain_fp64"] = plain_batched(sq, specs, circuits, "f64", args.plain_limit)
+    if dist.rank == 0 and not args.skip_cpu:
+        line["cpu_baseline"] = cpu_baseline_batched(args, specs)
+    return line
+
+
+def cpu_baseline_batched(args, specs, n_cap=18):
+    """t_PAR_CPU (FP32) on every 8th circuit, each on at most n_cap qubits, time scaled by 2^(n - n_cap)
+    and by 8 for the circuits not run."""
+    from oracle import circuit_lang as cl
+    from oracle import cpu
+
+    threads = os.cpu_count() or 1
+    kind = "reference" if cpu.ref_available("f32") else "port"
+    total = 0.0
+    sample = specs[::8]
+    for spec in sample:
+        full = spec.build(cl.Circuit())
+        t, cm, cv, m = full.as_arrays()
+        n = spec.qubits
+        ns = min(n, n_cap)
+        shift = n - ns
+        keep = [i for i in range(len(t)) if t[i] >= shift and (int(cm[i]) >> shift << shift) == int(cm[i])]
+        ops = (t[keep] - shift, cm[keep] >> shift, cv[keep] >> shift, m[keep])
+        s0 = cpu.basis_state(ns, spec.init_index >> shift, np.complex64)
+        if kind == "reference":
+            dt = ref_replay(ns, s0, ops, threads)
+        else:
+            t0 = time.perf_counter()
+            cpu.run_regions(s0, ns, ops, prec="f32", threads=threads)
+            dt = time.perf_counter() - t0
+        total += dt * (1 << shift)
+    total *= len(specs) / len(sample)
+    return {"value": round(len(specs) / total, 6), "unit": "circuits/s", "cores": threads, "kind": kind,
+            "sample": f"every 8th of the {len(specs)} circuits on t_PAR_CPU FP32, each on <= {n_cap} qubits, time "
+                      "scaled by state size and by 8"}
+
+
+# ---------------------------------------------------------------------------
 # served stream (continuous batching)
 # ---------------------------------------------------------------------------
 
@@ -459,8 +607,10 @@ def serve_step(sq, srv, reqs, items, rate_hz, rng, planned):
     return out, time.perf_counter() - t0
 
 
-def served_run(args, dist, sq, srv, steps_reqs, steps_items, planned, rng):
-    """Warm-up steps, then the timed steps (device-timed with a synchronize on both sides)."""
+def served_run(args, dist, sq, srv, steps_reqs, steps_items, planned, rng, rate=None):
+    """Warm-up steps, then the timed steps (device-timed with a synchronize on both sides); arrivals are
+    Poisson at `rate` requests/s (default args.rate; 0 = all of a step at once)."""
+    rate = args.rate if rate is None else rate
     for w in range(args.warmup):
         serve_step(sq, srv, steps_reqs[w], steps_items[w], 0, rng, planned)
     sq.synchronize()
@@ -471,7 +621,7 @@ def served_run(args, dist, sq, srv, steps_reqs, steps_items, planned, rng):
         with sq.Timer() as t:
             for s in range(args.steps):
                 res, _ = serve_step(sq, srv, steps_reqs[args.warmup + s], steps_items[args.warmup + s],
-                                    args.rate, rng, planned)
+                                    rate, rng, planned)
                 lat += [r["latency_s"] for r in res]
                 done += len(res)
                 assert all(r["status"] == 0 for r in res)
@@ -509,6 +659,15 @@ def workload_served(args, dist, sq):
                "path": "hgm_server_submit (host circuit: planned, op records uploaded) -> hgm_server_poll "
                        "(norm, argmax, pmax to host)",
                "latency_ms": lat2, "ms_per_step": round(ms2 / args.steps, 3)}
+    # Poisson arrivals at fractions of the measured capacity: throughput and latency per offered rate
+    sweep = []
+    if not args.skip_sweep and args.rate == 0:
+        for frac in (0.5, 0.8):
+            rate = frac * value / dist.world
+            v3, ms3, lat3, _, _ = served_run(args, dist, sq, srv, steps_reqs, steps_plans, True,
+                                             np.random.default_rng(11), rate=rate)
+            sweep.append({"offered_rate_hz": round(rate, 2), "fraction_of_capacity": frac,
+                          "circuits_per_s": round(v3, 4), "latency_ms": lat3})
     srv.close()
     del steps_plans
     # fidelity of the FP32 served results against FP64 reruns (first timed step)
@@ -525,6 +684,7 @@ def workload_served(args, dist, sq):
                       "(hgm_server_submit_plan); states initialised on the device",
                       "l2": "states up to 2 GiB; no flush (serving keeps states resident)"})
     line["latency_ms"] = latency
+    line["rate_sweep"] = sweep
     line["fidelity"] = fid
     line["plain_fp64"] = plain
     line["gpu_launches"] = launches
@@ -597,6 +757,33 @@ def served_roofline(sq, args, peak, peak_kind):
             "algorithmic_bytes_per_launch": 2 * S}
 
 
+def ref_replay(ns, s0, ops, threads):
+    """Replays (target, cmask, cval, matrix) ops on the reference's FP32 t_PAR_CPU engine as single-gate
+    steps from state s0; returns the seconds spent in the engine's execute calls."""
+    from oracle import cpu
+
+    r = cpu.RefDGM(ns, "f32")
+    r.set_state(s0)
+    r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
+    dt = 0.0
+    for i in range(len(ops[0])):
+        name = f"s{i}"
+        r.add_gate(name, ops[3][i])
+        tok = ["ID"] * ns
+        tgt = ns - 1 - int(ops[0][i])
+        cbits = int(ops[1][i])
+        for b in range(ns):
+            if (cbits >> b) & 1:
+                tok[ns - 1 - b] = "Control1(1)" if (int(ops[2][i]) >> b) & 1 else "Control1(0)"
+        tok[tgt] = f"Target1({name})" if cbits else name
+        r.set_function(",".join(tok), 1, True)
+        t0 = time.perf_counter()  # the engine's execution only, not the parse of the step
+        r.execute(1)
+        dt += time.perf_counter() - t0
+    r.close()
+    return dt
+
+
 def cpu_baseline_served(args, reqs, n_cap=20, op_cap=400):
     """The reference's t_PAR_CPU (FP32, unmodified) on the same request list, each request run on at most
     n_cap qubits and its first op_cap gates, the time scaled by 2^(n - n_cap) and total/op_cap gates."""
@@ -616,25 +803,7 @@ def cpu_baseline_served(args, reqs, n_cap=20, op_cap=400):
         ops = (t[keep] - shift, cm[keep] >> shift, cv[keep] >> shift, m[keep])
         s0 = cpu.basis_state(ns, spec.init_index >> shift, np.complex64)
         if kind == "reference":
-            r = cpu.RefDGM(ns, "f32")
-            r.set_state(s0)
-            r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
-            # replay the sampled ops through the reference engine as single-gate steps
-            t0 = time.perf_counter()
-            for i in range(len(keep)):
-                name = f"s{i}"
-                r.add_gate(name, ops[3][i])
-                tok = ["ID"] * ns
-                tgt = ns - 1 - int(ops[0][i])
-                cbits = int(ops[1][i])
-                for b in range(ns):
-                    if (cbits >> b) & 1:
-                        tok[ns - 1 - b] = "Control1(1)" if (int(ops[2][i]) >> b) & 1 else "Control1(0)"
-                tok[tgt] = f"Target1({name})" if cbits else name
-                r.set_function(",".join(tok), 1, True)
-                r.execute(1)
-            dt = time.perf_counter() - t0
-            r.close()
+            dt = ref_replay(ns, s0, ops, threads)
         else:
             t0 = time.perf_counter()
             cpu.run_regions(s0, ns, ops, prec="f32", threads=threads)
@@ -644,7 +813,8 @@ def cpu_baseline_served(args, reqs, n_cap=20, op_cap=400):
             "sample": f"{len(reqs)} requests of the served mix on t_PAR_CPU FP32; each run on <= {n_cap} qubits "
                       f"and its first <= {op_cap} gates, time scaled by state size and gate count"}
 
-WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": workload_grover}
+WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": workload_grover,
+             "batched": workload_batched}
 
 
 def base_line(args, dist, metric, value, unit, ms_step, dtype, config):
@@ -659,6 +829,7 @@ def reference_arm(args, dist):
         return None
     fn = {"layered": cpu_baseline_layered,
           "grover": lambda a: cpu_baseline_grover(a, a.qubits or GROVER_N, GROVER_MARK),
+          "batched": lambda a: cpu_baseline_batched(a, batched_specs(4242, a.requests or 512)),
           "served": lambda a: cpu_baseline_served(a, served_requests(1000 + a.warmup, a.requests or 48))}.get(args.workload)
     if fn is None:
         return {"impl": "reference", "unavailable": f"no reference timing for workload {args.workload}"}
@@ -690,12 +861,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-sweep", action="store_true", help="served: no Poisson rate sweep")
     ap.add_argument("--qubits", type=int, default=0, help="override the workload's qubit count (profiling runs)")
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")
     args = ap.parse_args()
     args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
                         "grover": "Grover iterations/s (26q FP64, marked index 42)",
+                        "batched": "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
                         "served": SERVED_METRIC}.get(args.workload, args.workload)
     dist = Dist()
     try:

@@ -51,6 +51,9 @@ int hgm_init(int device);
 int hgm_synchronize(void);
 /* Free / total device memory in bytes. */
 int hgm_mem_info(int64_t *free_bytes, int64_t *total_bytes);
+/* Page-locked host memory (cudaMallocHost), for asynchronous copies. */
+int hgm_pinned_alloc(int64_t bytes, void **out);
+void hgm_pinned_free(void *p);
 /* Number of kernel launches issued by this library since load. */
 int64_t hgm_kernel_launches(void);
 
@@ -175,9 +178,24 @@ int hgm_batch_add(hgm_batch *b, const hgm_circuit *c, int qubits, int64_t init_i
 int hgm_batch_finalize(hgm_batch *b);
 /* Launches the graph on `stream` (0 = library stream); asynchronous. */
 int hgm_batch_run(hgm_batch *b, void *stream);
+/* Autotuner: re-plans the batch for every tile size (warp_bits 0..3) and
+ * every count of always-resident low index bits (3..5), times two graph
+ * replays of each, and leaves the batch finalized with the fastest; reports
+ * the choice and its time per run (ms). */
+int hgm_batch_autotune(hgm_batch *b, void *stream, int *warp_bits, int *low_bits, double *ms);
+/* Sets every job's initial basis index for the next runs (an asynchronous
+ * copy of njobs int64 values on `stream`; pinned memory keeps it so). */
+int hgm_batch_set_inputs(hgm_batch *b, const int64_t *init_index, void *stream);
+/* Copies every job's state (the arena: jobs back to back in job order, each
+ * 2^n amplitudes) to `host` (exactly the arena's bytes; asynchronous on
+ * `stream` when `host` is pinned). */
+int hgm_batch_download(hgm_batch *b, void *host, int64_t bytes, void *stream);
 /* After a run has completed: HGM_ERR_TIMEOUT if a tile gave up waiting. */
 int hgm_batch_check(hgm_batch *b);
-int hgm_batch_size(const hgm_batch *b, int *jobs, int64_t *tasks, int64_t *items, int64_t *arena_bytes);
+/* pass_bytes: the algorithmic bytes of one run, a read and a write of a
+ * state per pass (per task). */
+int hgm_batch_size(const hgm_batch *b, int *jobs, int64_t *tasks, int64_t *items, int64_t *arena_bytes,
+                   int64_t *pass_bytes);
 /* A view of one job's state (owned by the batch; hgm_state_free ignores it). */
 hgm_state *hgm_batch_state(hgm_batch *b, int job);
 

@@ -89,8 +89,13 @@ def _load():
         "hgm_batch_add": ([vp, vp, i, i64, P(i)], i),
         "hgm_batch_finalize": ([vp], i),
         "hgm_batch_run": ([vp, vp], i),
+        "hgm_batch_autotune": ([vp, vp, P(i), P(i), P(C.c_double)], i),
+        "hgm_batch_set_inputs": ([vp, P(i64), vp], i),
+        "hgm_batch_download": ([vp, vp, i64, vp], i),
+        "hgm_pinned_alloc": ([i64, P(vp)], i),
+        "hgm_pinned_free": ([vp], None),
         "hgm_batch_check": ([vp], i),
-        "hgm_batch_size": ([vp, P(i), P(i64), P(i64), P(i64)], i),
+        "hgm_batch_size": ([vp, P(i), P(i64), P(i64), P(i64), P(i64)], i),
         "hgm_batch_state": ([vp, i], vp),
         "hgm_server_default_opts": ([P(ServerOpts), i], None),
         "hgm_server_create": ([P(ServerOpts), P(vp)], i),

@@ -168,6 +168,7 @@ struct BatchJob {
 struct Batch {
     int precision = HGM_F64;
     int warp_bits = 2;
+    int low_bits = -1;      // the planner's default when negative
     std::vector<BatchJob> jobs;
     bool finalized = false;
     std::vector<BatchTask> tasks;
@@ -184,11 +185,27 @@ struct Batch {
     cudaGraphExec_t graph = nullptr;
     cudaStream_t stream = nullptr;
     std::vector<State> views;
-    ~Batch() {
+    ~Batch() { release(); }
+    // Drops everything finalize built (plans, arena, tables, graph); the
+    // circuits stay, so the batch can be finalized again with other settings.
+    void release() {
         if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
         for (void *p : {(void *)arena, (void *)d_tasks, (void *)d_next, (void *)d_done, (void *)d_error,
                         (void *)d_offsets, (void *)d_init})
             if (p) cudaFree(p);
+        arena = nullptr;
+        d_tasks = nullptr;
+        d_next = nullptr;
+        d_done = nullptr;
+        d_error = nullptr;
+        d_offsets = d_init = nullptr;
+        for (BatchJob &j : jobs) j.plan.reset();
+        tasks.clear();
+        views.clear();
+        total_items = 0;
+        arena_bytes = 0;
+        finalized = false;
     }
 };
 
@@ -244,6 +261,7 @@ int batch_finalize(Batch *b) {
         hgm_plan_default_opts(&o, b->precision);
         o.renorm_every = 0;
         o.warp_bits = b->warp_bits;
+        o.low_bits = b->low_bits;
         j.plan.reset(new Plan());
         // a state smaller than one tile runs whole in one CTA's shared memory
         int rc = build_plan(j.ops, j.n, o, j.plan.get(), j.n < K);
@@ -393,6 +411,82 @@ int hgm_batch_run(hgm_batch *bb, void *stream) {
     return cuda_err(e, "batch graph launch");
 }
 
+int hgm_batch_autotune(hgm_batch *bb, void *stream, int *warp_bits, int *low_bits, double *ms) {
+    Batch *b = reinterpret_cast<Batch *>(bb);
+    if (!b) return fail(HGM_ERR_INVALID, "null batch");
+    if (b->jobs.empty()) return fail(HGM_ERR_INVALID, "empty batch");
+    cudaStream_t st = stream ? (cudaStream_t)stream : (cudaStream_t)default_stream();
+    // earlier runs of this batch must be done before its buffers are dropped
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    cudaStreamSynchronize(st);
+    cudaEvent_t e0, e1;
+    int rc;
+    if ((rc = cuda_err(cudaEventCreate(&e0), "autotune event")) || (rc = cuda_err(cudaEventCreate(&e1), "autotune event")))
+        return rc;
+    // tile size (warps per CTA) x always-resident low index bits: the two
+    // settings that decide a plan's pass count and its tile work
+    int best_w = -1, best_l = -1;
+    float best = 0.f;
+    const int lows[3] = {3, 4, 5};
+    for (int w = 0; w <= 3 && !rc; w++) {
+        for (int li = 0; li < 3 && !rc; li++) {
+            b->release();
+            b->warp_bits = w;
+            b->low_bits = lows[li];
+            if ((rc = batch_finalize(b))) break;
+            cudaGraphLaunch(b->graph, st);  // warm-up
+            cudaEventRecord(e0, st);
+            for (int k = 0; k < 2; k++) cudaGraphLaunch(b->graph, st);
+            cudaEventRecord(e1, st);
+            if ((rc = cuda_err(cudaEventSynchronize(e1), "autotune run"))) break;
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            t *= 0.5f;
+            if (best_w < 0 || t < best) {
+                best = t;
+                best_w = w;
+                best_l = lows[li];
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    b->release();
+    b->warp_bits = best_w;
+    b->low_bits = best_l;
+    if ((rc = batch_finalize(b))) return rc;
+    if (warp_bits) *warp_bits = best_w;
+    if (low_bits) *low_bits = best_l;
+    if (ms) *ms = best;
+    return HGM_OK;
+}
+
+int hgm_batch_set_inputs(hgm_batch *bb, const int64_t *init_index, void *stream) {
+    Batch *b = reinterpret_cast<Batch *>(bb);
+    if (!b || !init_index) return fail(HGM_ERR_INVALID, "null argument");
+    int rc = batch_finalize(b);
+    if (rc) return rc;
+    for (size_t j = 0; j < b->jobs.size(); j++)
+        if (init_index[j] < 0 || init_index[j] >= (1ll << b->jobs[j].n))
+            return fail(HGM_ERR_INVALID, "job %zu: initial index outside its state", j);
+    for (size_t j = 0; j < b->jobs.size(); j++) b->jobs[j].init_index = init_index[j];
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    return cuda_err(cudaMemcpyAsync(b->d_init, init_index, b->jobs.size() * sizeof(long long), cudaMemcpyHostToDevice, st),
+                    "batch inputs");
+}
+
+int hgm_batch_download(hgm_batch *bb, void *host, int64_t bytes, void *stream) {
+    Batch *b = reinterpret_cast<Batch *>(bb);
+    if (!b || !host) return fail(HGM_ERR_INVALID, "null argument");
+    if (!b->finalized) return fail(HGM_ERR_INVALID, "batch not finalized");
+    if (bytes != (int64_t)b->arena_bytes)
+        return fail(HGM_ERR_INVALID, "host buffer of %lld bytes for an arena of %lld", (long long)bytes,
+                    (long long)b->arena_bytes);
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    return cuda_err(cudaMemcpyAsync(host, b->arena, b->arena_bytes, cudaMemcpyDeviceToHost, st), "batch download");
+}
+
 int hgm_batch_check(hgm_batch *bb) {
     Batch *b = reinterpret_cast<Batch *>(bb);
     if (!b || !b->finalized) return fail(HGM_ERR_INVALID, "batch not run");
@@ -402,13 +496,20 @@ int hgm_batch_check(hgm_batch *bb) {
     return err ? fail(HGM_ERR_TIMEOUT, "a batched tile gave up waiting for its previous pass") : HGM_OK;
 }
 
-int hgm_batch_size(const hgm_batch *bb, int *jobs, int64_t *tasks, int64_t *items, int64_t *arena_bytes) {
+int hgm_batch_size(const hgm_batch *bb, int *jobs, int64_t *tasks, int64_t *items, int64_t *arena_bytes,
+                   int64_t *pass_bytes) {
     const Batch *b = reinterpret_cast<const Batch *>(bb);
     if (!b) return fail(HGM_ERR_INVALID, "null batch");
     if (jobs) *jobs = (int)b->jobs.size();
     if (tasks) *tasks = (int64_t)b->tasks.size();
     if (items) *items = b->total_items;
     if (arena_bytes) *arena_bytes = (int64_t)b->arena_bytes;
+    if (pass_bytes) {  // one read and one write of a state per pass (per shared-memory task)
+        const int64_t amp = b->precision == HGM_F64 ? 16 : 8;
+        int64_t t = 0;
+        for (const BatchTask &k : b->tasks) t += 2 * amp * (int64_t(1) << k.n);
+        *pass_bytes = t;
+    }
     return HGM_OK;
 }
 

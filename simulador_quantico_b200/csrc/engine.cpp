@@ -48,6 +48,16 @@ int hgm_synchronize(void) {
     return e == cudaSuccess ? HGM_OK : cuda_fail(e, "cudaDeviceSynchronize");
 }
 
+int hgm_pinned_alloc(int64_t bytes, void **out) {
+    if (!out || bytes <= 0) return fail(HGM_ERR_INVALID, "bad pinned allocation request");
+    cudaError_t e = cudaMallocHost(out, (size_t)bytes);
+    return e == cudaSuccess ? HGM_OK : cuda_fail(e, "cudaMallocHost");
+}
+
+void hgm_pinned_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+
 int hgm_mem_info(int64_t *free_bytes, int64_t *total_bytes) {
     size_t f = 0, t = 0;
     cudaError_t e = cudaMemGetInfo(&f, &t);

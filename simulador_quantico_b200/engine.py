@@ -242,13 +242,31 @@ class Batch:
         check(lib.hgm_batch_run(self.h, stream))
         return self
 
+    def autotune(self, stream=None) -> dict:
+        """Picks the tile size and resident low bits by timing graph replays."""
+        w, lo, ms = C.c_int(), C.c_int(), C.c_double()
+        check(lib.hgm_batch_autotune(self.h, stream, C.byref(w), C.byref(lo), C.byref(ms)))
+        return dict(warp_bits=w.value, low_bits=lo.value, ms=ms.value)
+
+    def set_inputs(self, init_index, stream=None):
+        """Every job's initial basis index for the next runs (int64 array, one per job)."""
+        a = np.ascontiguousarray(init_index, dtype=np.int64)
+        check(lib.hgm_batch_set_inputs(self.h, a.ctypes.data_as(C.POINTER(C.c_int64)), stream))
+        self._inputs = a  # the copy is asynchronous: keep the buffer alive
+        return self
+
+    def download(self, host: "PinnedArray", stream=None):
+        """Every job's state, back to back in job order, into `host` (asynchronous)."""
+        check(lib.hgm_batch_download(self.h, C.c_void_p(host.ptr), host.nbytes, stream))
+        return self
+
     def check(self):
         check(lib.hgm_batch_check(self.h))
 
     def size(self) -> dict:
-        j, t, it, ab = C.c_int(), C.c_int64(), C.c_int64(), C.c_int64()
-        check(lib.hgm_batch_size(self.h, C.byref(j), C.byref(t), C.byref(it), C.byref(ab)))
-        return dict(jobs=j.value, tasks=t.value, items=it.value, arena_bytes=ab.value)
+        j, t, it, ab, pb = C.c_int(), C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib.hgm_batch_size(self.h, C.byref(j), C.byref(t), C.byref(it), C.byref(ab), C.byref(pb)))
+        return dict(jobs=j.value, tasks=t.value, items=it.value, arena_bytes=ab.value, pass_bytes=pb.value)
 
     def state(self, job: int) -> State:
         h = lib.hgm_batch_state(self.h, job)
@@ -411,3 +429,23 @@ class DGM:
 
     def host_state(self):
         return self.state.download()
+
+
+class PinnedArray:
+    """A numpy array in page-locked host memory (hgm_pinned_alloc)."""
+
+    def __init__(self, shape, dtype):
+        init()
+        dt = np.dtype(dtype)
+        n = int(np.prod(shape)) * dt.itemsize
+        p = C.c_void_p()
+        check(lib.hgm_pinned_alloc(max(n, 1), C.byref(p)))
+        self.ptr, self.nbytes = p.value, n
+        buf = (C.c_char * max(n, 1)).from_address(self.ptr)
+        self.array = np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self.array = None
+            lib.hgm_pinned_free(C.c_void_p(self.ptr))
+            self.ptr = None

@@ -65,3 +65,46 @@ def test_batch_size_report(sq):
     s = b.size()
     assert s["jobs"] == 8 and s["tasks"] >= 8 and s["items"] >= s["tasks"]
     assert s["arena_bytes"] == sum(16 << spec.qubits for spec in specs)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_batch_autotune_keeps_results(sq, prec):
+    """The autotuner tries every tile size and resident-low-bit count and
+    leaves the batch finalized with the fastest; results still match the
+    oracle afterwards."""
+    specs = mixed_specs(41, 12, 8, 14)
+    b = sq.Batch(prec, 2)
+    for spec in specs:
+        b.add(spec.build(sq.Circuit()), spec.qubits, spec.init_index)
+    b.finalize().run()  # a finalized, already-run batch may be retuned
+    pick = b.autotune()
+    assert 0 <= pick["warp_bits"] <= 3 and pick["low_bits"] in (3, 4, 5) and pick["ms"] > 0
+    b.run()
+    sq.synchronize()
+    b.check()
+    for j, spec in enumerate(specs):
+        got = b.state(j).download()
+        assert np.abs(got - oracle_state(spec, prec)).max() < (TOL_F64 if prec == "f64" else TOL_F32), spec.name
+
+
+def test_batch_set_inputs(sq):
+    """New initial basis states per run (hgm_batch_set_inputs) give the
+    results of those inputs; an index outside a job's state is refused."""
+    rng = np.random.default_rng(9)
+    ns = [int(x) for x in rng.integers(9, 14, 10)]
+    specs = [wl.qft(n, 0) for n in ns]
+    b = sq.Batch("f64", 1)
+    for spec in specs:
+        b.add(spec.build(sq.Circuit()), spec.qubits, 0)
+    b.finalize()
+    for rep in range(2):
+        inputs = np.array([int(rng.integers(1 << n)) for n in ns], dtype=np.int64)
+        b.set_inputs(inputs).run()
+        sq.synchronize()
+        for j, (spec, x) in enumerate(zip(specs, inputs)):
+            spec_x = wl.qft(spec.qubits, int(x))
+            assert np.abs(b.state(j).download() - oracle_state(spec_x, "f64")).max() < TOL_F64, (rep, j)
+    bad = np.zeros(len(ns), dtype=np.int64)
+    bad[3] = 1 << ns[3]
+    with pytest.raises(sq.HgmError):
+        b.set_inputs(bad)
