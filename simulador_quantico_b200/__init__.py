@@ -7,9 +7,9 @@ importing this package without them raises ImportError (there is no CPU
 fallback).
 """
 from .engine import (DGM, T_CPU, T_GPU, T_HYBRID, T_PAR_CPU, Batch, Circuit, PinnedArray, Plan, Server, State, Timer,
-                     init, kernel_launches, plan_opts, synchronize)
+                     init, kernel_launches, mem_info, plan_opts, synchronize)
 from ._lib import HGM_F32, HGM_F64, HgmError, load_dropin
 
 __all__ = ["DGM", "Batch", "Server", "Circuit", "PinnedArray", "Plan", "State", "Timer", "init", "synchronize",
-           "kernel_launches", "plan_opts",
+           "kernel_launches", "mem_info", "plan_opts",
            "load_dropin", "HgmError", "HGM_F32", "HGM_F64", "T_CPU", "T_PAR_CPU", "T_GPU", "T_HYBRID"]

@@ -540,40 +540,104 @@ __global__ void marginal_final(const double *pbest, const long long *ibest, int 
     }
 }
 
-int launch_argmax_async(State *s, uint64_t mask, double *pbest, long long *ibest, double *out, void *stream) {
-    cudaStream_t st = (cudaStream_t)stream;
+// Marginal argmax for a small mask (2^m <= RED_BLOCKS values): block b
+// handles value x = b / nch over the (b % nch)-th chunk of the complement
+// indices, its threads striding over the chunk, and writes that chunk's
+// probability; marginal_chunks_final sums each value's chunks in order.  With
+// the per-value kernel above, a thread would walk all 2^(n-m) complement
+// indices of its value alone (minutes for a few-bit mask on a 32-qubit state).
+template <typename Real>
+__global__ void __launch_bounds__(RED_THREADS) marginal_chunk_kernel(const typename V2<Real>::T *__restrict__ s, int n,
+                                                                      unsigned long long mask, int nch,
+                                                                      double *partial) {
+    const unsigned long long comp = ~mask & ((n >= 64) ? ~0ull : ((1ull << n) - 1));
+    const long long C = 1ll << (n - __popcll(mask));
+    const long long x = blockIdx.x / nch, chunk = blockIdx.x % nch;
+    const long long cs = (C + nch - 1) / nch, c0 = chunk * cs, c1 = c0 + cs < C ? c0 + cs : C;
+    unsigned long long base = 0, src = (unsigned long long)x, mm = mask;
+    while (mm) {
+        const int g = __ffsll((long long)mm) - 1;
+        mm &= mm - 1;
+        base |= (src & 1ull) << g;
+        src >>= 1;
+    }
+    double p = 0.0;
+    for (long long c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        unsigned long long idx = base, cv = (unsigned long long)c, cm = comp;
+        while (cm) {
+            const int g = __ffsll((long long)cm) - 1;
+            cm &= cm - 1;
+            idx |= (cv & 1ull) << g;
+            cv >>= 1;
+        }
+        const typename V2<Real>::T v = s[idx];
+        p += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    p = warp_sum(p);
+    __shared__ double sh[RED_THREADS / 32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = p;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < RED_THREADS / 32; k++) t += sh[k];
+        partial[blockIdx.x] = t;
+    }
+}
+
+__global__ void marginal_chunks_final(const double *partial, long long M, int nch, double *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double b = -1.0;
+        long long bi = 0;
+        for (long long x = 0; x < M; x++) {
+            double p = 0.0;
+            for (int k = 0; k < nch; k++) p += partial[x * nch + k];
+            if (p > b) {  // lowest value on ties
+                b = p;
+                bi = x;
+            }
+        }
+        out[0] = b;
+        out[1] = (double)bi;
+    }
+}
+
+// Queues the marginal argmax of `mask` over state s: its probability and
+// value land in out[0], out[1].  Scratch: pbest / ibest of RED_BLOCKS entries.
+static int queue_marginal(State *s, uint64_t mask, double *pbest, long long *ibest, double *out, cudaStream_t st) {
     const int n = s->qubits;
     if (n < 64 && (mask >> n)) return fail(HGM_ERR_INVALID, "mask beyond state bits");
     const int m = __builtin_popcountll(mask);
     const long long M = 1ll << m;
-    unsigned g = (unsigned)((M + RED_THREADS - 1) / RED_THREADS);
-    if (g > RED_BLOCKS) g = RED_BLOCKS;
-    if (g < 1) g = 1;
-    if (s->precision == HGM_F64)
-        marginal_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, m, pbest, ibest);
-    else
-        marginal_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, m, pbest, ibest);
-    marginal_final<<<1, 32, 0, st>>>(pbest, ibest, (int)g, out);
+    if (M <= RED_BLOCKS) {
+        const int nch = (int)(RED_BLOCKS / M);
+        const unsigned g = (unsigned)(M * nch);
+        if (s->precision == HGM_F64)
+            marginal_chunk_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, nch, pbest);
+        else
+            marginal_chunk_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, nch, pbest);
+        marginal_chunks_final<<<1, 32, 0, st>>>(pbest, M, nch, out);
+    } else {
+        unsigned g = (unsigned)((M + RED_THREADS - 1) / RED_THREADS);
+        if (g > RED_BLOCKS) g = RED_BLOCKS;
+        if (s->precision == HGM_F64)
+            marginal_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, m, pbest, ibest);
+        else
+            marginal_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, m, pbest, ibest);
+        marginal_final<<<1, 32, 0, st>>>(pbest, ibest, (int)g, out);
+    }
     count_launch(2);
     return check("argmax launch");
+}
+
+int launch_argmax_async(State *s, uint64_t mask, double *pbest, long long *ibest, double *out, void *stream) {
+    return queue_marginal(s, mask, pbest, ibest, out, (cudaStream_t)stream);
 }
 
 int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *stream) {
     cudaStream_t st = pick(stream);
     if (!st) return HGM_ERR_CUDA;
-    const int n = s->qubits;
-    if (n < 64 && (mask >> n)) return fail(HGM_ERR_INVALID, "mask beyond state bits");
-    const int m = __builtin_popcountll(mask);
-    const long long M = 1ll << m;
-    unsigned g = (unsigned)((M + RED_THREADS - 1) / RED_THREADS);
-    if (g > RED_BLOCKS) g = RED_BLOCKS;
-    if (g < 1) g = 1;
-    if (s->precision == HGM_F64)
-        marginal_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, m, g_ctx.partials, g_ctx.partial_idx);
-    else
-        marginal_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, m, g_ctx.partials, g_ctx.partial_idx);
-    marginal_final<<<1, 32, 0, st>>>(g_ctx.partials, g_ctx.partial_idx, (int)g, g_ctx.result);
-    count_launch(2);
+    const int rc = queue_marginal(s, mask, g_ctx.partials, g_ctx.partial_idx, g_ctx.result, st);
+    if (rc) return rc;
     cudaMemcpyAsync(g_ctx.host_result, g_ctx.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "marginal argmax: %s", cudaGetErrorString(e));

@@ -95,7 +95,12 @@ struct Server {
     std::string error_msg;  // the worker's message for `error`, reported by hgm_server_poll
 
     ~Server() {
-        stop = true;
+        {
+            // under the mutex: a thread between its predicate check and its
+            // wait would otherwise miss the wake-up and never return
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
         plan_cv.notify_all();
         cv.notify_all();
         for (std::thread &t : planners)
@@ -187,7 +192,7 @@ struct Server {
             Request *r = nullptr;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                plan_cv.wait(lk, [this] { return stop || !to_plan.empty(); });
+                while (!stop && to_plan.empty()) plan_cv.wait_for(lk, std::chrono::milliseconds(100));
                 if (stop) return;
                 r = to_plan.front();
                 to_plan.pop_front();

@@ -88,7 +88,8 @@ class Circuit:
         return t, cm, cv, mm[..., 0] + 1j * mm[..., 1]
 
     def ref_pts(self, precision="f64"):
-        """NULL-terminated PT** in the reference's struct layout."""
+        """NULL-terminated PT** in the reference's struct layout.  The arrays
+        belong to this circuit: the pointer is valid while the circuit lives."""
         p = lib.hgm_circuit_ref_pts(self.h, PREC[precision])
         if not p:
             raise _lib.HgmError(1, _lib.last_error())
@@ -345,6 +346,14 @@ class Server:
 
 def synchronize():
     check(lib.hgm_synchronize())
+
+
+def mem_info():
+    """(free, total) device memory in bytes."""
+    init()
+    f, t = C.c_int64(), C.c_int64()
+    check(lib.hgm_mem_info(C.byref(f), C.byref(t)))
+    return f.value, t.value
 
 
 def kernel_launches() -> int:
