@@ -205,6 +205,8 @@ def workload_layered(args, dist, sq):
     pass_ms = ms_step / stats["passes"]
     achieved = 2 * S / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = hbm_peak()
+    # outside the timed region: the unitary circuit keeps the norm (FP64 reduction on the device)
+    norm = st.norm()
     # end to end through the reference's C-ABI with host buffers (1 step)
     e2e = e2e_layered(dist, sq, spec, n, prec) if not args.skip_e2e else None
     st.free()
@@ -223,6 +225,7 @@ def workload_layered(args, dist, sq):
                         "algorithmic_bytes_per_launch": 2 * S}
     line["gpu_launches"] = launches
     line["clocks"] = clk.summary()
+    line["norm_after"] = {"value": norm, "ok": bool(abs(norm - 1.0) < (1e-9 if prec == "f64" else 1e-3))}
     line["e2e"] = e2e
     if dist.rank == 0 and not args.skip_cpu:
         line["cpu_baseline"] = cpu_baseline_layered(args)

@@ -10,9 +10,11 @@
 #                               (float complex -> double complex, crealf/
 #                               cimagf/cpowf -> creal/cimag/cpow, float
 #                               accumulators -> double)
-#   oracle/_ref/general_ref_{f32,f64}.out, grover_ref_{f32,f64}.out
+#   oracle/_ref/general_ref_{f32,f64}.out, grover_ref_{f32,f64}.out,
+#   oracle/_ref/shor_ref_{f32,f64}.out
 #                               the reference CLIs on the stub GPU backend
 #   oracle/_ref/general_b200_{f32,f64}.out, grover_b200_{f32,f64}.out,
+#   oracle/_ref/shor_b200_{f32,f64}.out,
 #   oracle/_ref/libref_dropin_{f32,f64}.so
 #                               the same reference objects with the GPU
 #                               backend replaced at link time by
@@ -41,7 +43,7 @@ fi
 mkdir -p "$OUT"
 CXX="${REF_CXX:-g++}"
 ENGINE_FILES="dgm_core dgm_parser dgm_cpu_exec dgm_par_exec"
-PLAIN_FILES="common gates lib_general lib_grover cli_common kernel_stub"
+PLAIN_FILES="common gates lib_general lib_grover lib_shor lib_shor_number_theory lib_shor_circuits cli_common kernel_stub"
 
 build_variant() {
     local prec="$1"        # f32 | f64
@@ -72,16 +74,19 @@ build_variant() {
     done
     $CXX $inc -fPIC -fopenmp -c "$work/src/cli/general.cpp" -o "$work/obj/general.o"
     $CXX $inc -fPIC -fopenmp -c "$work/src/cli/grover.cpp" -o "$work/obj/grover.o"
+    $CXX $inc -fPIC -fopenmp -c "$work/src/cli/shor.cpp" -o "$work/obj/shor.o"
     $CXX $inc -I"$work/include" -DREF_REAL="$real" -fPIC -O2 -fopenmp \
         -c "$HERE/ref_harness.cpp" -o "$work/obj/ref_harness.o"
 
     local core=""
-    for f in dgm_core dgm_parser dgm_cpu_exec dgm_par_exec common gates lib_general lib_grover cli_common; do
+    for f in dgm_core dgm_parser dgm_cpu_exec dgm_par_exec common gates lib_general lib_grover lib_shor \
+             lib_shor_number_theory lib_shor_circuits cli_common; do
         core="$core $work/obj/$f.o"
     done
     $CXX -shared -o "$OUT/libref_$prec.so" $core "$work/obj/kernel_stub.o" "$work/obj/ref_harness.o" -fopenmp
     $CXX -o "$OUT/general_ref_$prec.out" "$work/obj/general.o" $core "$work/obj/kernel_stub.o" -fopenmp
     $CXX -o "$OUT/grover_ref_$prec.out" "$work/obj/grover.o" $core "$work/obj/kernel_stub.o" -fopenmp
+    $CXX -o "$OUT/shor_ref_$prec.out" "$work/obj/shor.o" $core "$work/obj/kernel_stub.o" -fopenmp
 
     # Link-time replacement of the GPU backend (makefile:51-61) by the
     # product's drop-in library, when it has been built.
@@ -93,6 +98,8 @@ build_variant() {
         $CXX -o "$OUT/general_b200_$prec.out" "$work/obj/general.o" $core \
             -L"$DROPIN_DIR" -lhgm_dropin_$prec $rp -fopenmp
         $CXX -o "$OUT/grover_b200_$prec.out" "$work/obj/grover.o" $core \
+            -L"$DROPIN_DIR" -lhgm_dropin_$prec $rp -fopenmp
+        $CXX -o "$OUT/shor_b200_$prec.out" "$work/obj/shor.o" $core \
             -L"$DROPIN_DIR" -lhgm_dropin_$prec $rp -fopenmp
     fi
     rm -rf "$work"

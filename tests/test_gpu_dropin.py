@@ -106,3 +106,22 @@ def test_grover_out_unchanged(sq):
         assert out.returncode == 0, out.stdout + out.stderr
         hits += "Found value: 10" in out.stdout
     assert hits >= 2
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_shor_out_unchanged(sq, prec):
+    """tests/smoke_test.sh:114-120: shor.out 15 2 1 (t_GPU) runs without a
+    crash and finds the factors of 57 at least once in 16 runs (Shor's
+    period finding is probabilistic; 2n executeFunction + measure rounds,
+    each a GpuExecutionWrapper call on the host state)."""
+    exe = REF / f"shor_b200_{prec}.out"
+    if not exe.exists():
+        pytest.skip("reference CLIs not linked (oracle/build_ref.sh)")
+    found = 0
+    for _ in range(16):
+        out = subprocess.run([str(exe), "15", "2", "1"], capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0 and "Time:" in out.stdout, out.stdout + out.stderr
+        if "Found factors: 3 -- 19" in out.stdout or "Found factors: 19 -- 3" in out.stdout:
+            found += 1
+            break
+    assert found >= 1
