@@ -9,6 +9,8 @@ Workloads (synthetic, seeded; see DESIGN.md for the shapes):
   batched  512 circuits of 10-22 qubits (half QFTs, half random layered) in
            one persistent kernel replayed from a CUDA graph, FP32 (value) and
            FP64, autotuned; metric batched circuits/s
+  hadamard one gate layer, H on every qubit of a 30-qubit FP64 state (the
+           Hadamard benchmark's shape); metric gate-layers/s
   layered  a 30-qubit, 40-layer random Rz/Ry + CNOT circuit in FP64; metric
            gate-layers/s (one step = the whole circuit)
   grover   Grover search, 26 qubits FP64, marked index 42 (the phase
@@ -284,6 +286,105 @@ def cpu_baseline_layered(args, kind="reference"):
             "sample": f"{layers_s} layers at {n_s} qubits FP64 t_PAR_CPU ({dt:.2f} s), scaled x{1 << (30 - n_s)} "
                       f"to 30 qubits"}
 
+
+
+# ---------------------------------------------------------------------------
+# one gate layer (config 1's shape, H on every qubit) at 30 qubits FP64
+# ---------------------------------------------------------------------------
+
+def workload_hadamard(args, dist, sq):
+    """H on every qubit of a 30-qubit FP64 state: a gate layer with few gates per pass, so the pass kernel
+    is bound by HBM rather than by its FP64 pipe.  One step = the layer."""
+    from simulador_quantico_b200 import workloads as wl
+
+    n = args.qubits or 30
+    spec = wl.hadamard_benchmark(n, iterations=1)
+    c = spec.build(sq.Circuit())
+    plan = sq.Plan(c, n, "f64")
+    stats = plan.stats()
+    st = sq.State(n, "f64").set_basis(0)
+
+    def step():
+        st.execute(plan)
+
+    with ClockSampler(dist.local_rank) as clk:
+        ms, launches = run_timed(dist, sq, step, args.steps, args.warmup)
+    ms_step = dist.max(ms / args.steps)
+    S = st.nbytes
+    value = dist.world / (ms_step * 1e-3)
+    achieved = stats["passes"] * 2 * S / (ms_step * 1e-3) / 1e9
+    # outside the timed region: after an odd number of layers every amplitude is 2^(-n/2)
+    runs = args.warmup + args.steps
+    p0 = st.prob_one(0)
+    st.free()
+    peak, peak_kind = hbm_peak()
+    line = base_line(args, dist, "gate-layers/s (H on every qubit, 30q FP64)", value, "layers/s", ms_step, "f64",
+                     {"workload": f"hadamard-layer-{n}q-fp64", "qubits": n, "gates_per_layer": n,
+                      "passes_per_step": stats["passes"], "state_bytes": S,
+                      "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"})
+    line["check"] = {"layers_applied": runs, "prob_one_bit0": p0,
+                     "ok": bool(abs(p0 - (0.5 if runs % 2 else 0.0)) < 1e-9)}
+    line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4),
+                        "traffic": round(TRAFFIC_OVER_ALGO["f64"] * 2 * S / 1e9, 3), "traffic_unit": "GB per launch",
+                        "traffic_source": "ncu capture of the 26-qubit FP64 layered case, scaled to this state size",
+                        "peak_source": peak_kind,
+                        "kernel": "pass_kernel<double,%d,%d>" % (stats["reg_bits"], stats["warp_bits"]),
+                        "algorithmic_bytes_per_launch": 2 * S}
+    line["gpu_launches"] = launches
+    line["clocks"] = clk.summary()
+    line["e2e"] = e2e_hadamard(dist, sq, c, n) if not args.skip_e2e else None
+    if dist.rank == 0 and not args.skip_cpu:
+        line["cpu_baseline"] = cpu_baseline_hadamard(args, n)
+    return line
+
+
+def e2e_hadamard(dist, sq, c, n):
+    """The layer through the reference's C-ABI: GpuExecutionWrapper on a host state (16 GiB each way)."""
+    L = sq.load_dropin("f64")
+    L.setDevice(dist.local_rank)
+    pts = c.ref_pts("f64")
+    host = np.zeros(1 << n, dtype=np.complex128)
+    host[0] = 1.0
+    t0 = time.perf_counter()
+    L.GpuExecutionWrapper(host.ctypes.data, pts, n, 4, 8, 1, 64, 2, 1)
+    dt = dist.max(time.perf_counter() - t0)
+    ok = abs(host[0].real - 2.0 ** (-n / 2)) < 1e-12 and abs(host[-1].real - 2.0 ** (-n / 2)) < 1e-12
+    return {"value": round(dist.world / dt, 4), "unit": "layers/s", "h2d_bytes_per_step": int(host.nbytes),
+            "d2h_bytes_per_step": int(host.nbytes), "path": "GpuExecutionWrapper (reference C-ABI), host state",
+            "seconds": round(dt, 3), "amplitudes_ok": bool(ok)}
+
+
+def cpu_baseline_hadamard(args, n, n_s=26):
+    """t_PAR_CPU: the layer at 26 qubits, scaled by 2^(n-26)."""
+    from oracle import cpu
+    from simulador_quantico_b200 import workloads as wl
+
+    threads = os.cpu_count() or 1
+    spec = wl.hadamard_benchmark(n_s, iterations=1)
+    if cpu.ref_available("f64"):
+        r = cpu.RefDGM(n_s, "f64")
+        r.set_memory_value(0)
+        for steps, it, reset in spec.calls:
+            r.set_function(steps, it, reset)
+        r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
+        t0 = time.perf_counter()
+        r.execute(1)
+        dt = time.perf_counter() - t0
+        r.close()
+        kind = "reference"
+    else:
+        from oracle import circuit_lang as cl
+
+        ops = spec.build(cl.Circuit()).as_arrays()
+        s0 = cpu.basis_state(n_s, 0)
+        t0 = time.perf_counter()
+        cpu.run_regions(s0, n_s, ops, threads=threads)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    per = dt * (1 << (n - n_s))
+    return {"value": round(1.0 / per, 6), "unit": "layers/s", "cores": threads, "kind": kind,
+            "sample": f"the layer at {n_s} qubits FP64 t_PAR_CPU ({dt:.2f} s), scaled x{1 << (n - n_s)} to {n} qubits"}
 
 
 # ---------------------------------------------------------------------------
@@ -817,7 +918,7 @@ def cpu_baseline_served(args, reqs, n_cap=20, op_cap=400):
                       f"and its first <= {op_cap} gates, time scaled by state size and gate count"}
 
 WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": workload_grover,
-             "batched": workload_batched}
+             "batched": workload_batched, "hadamard": workload_hadamard}
 
 
 def base_line(args, dist, metric, value, unit, ms_step, dtype, config):
@@ -832,6 +933,7 @@ def reference_arm(args, dist):
         return None
     fn = {"layered": cpu_baseline_layered,
           "grover": lambda a: cpu_baseline_grover(a, a.qubits or GROVER_N, GROVER_MARK),
+          "hadamard": lambda a: cpu_baseline_hadamard(a, a.qubits or 30),
           "batched": lambda a: cpu_baseline_batched(a, batched_specs(4242, a.requests or 512)),
           "served": lambda a: cpu_baseline_served(a, served_requests(1000 + a.warmup, a.requests or 48))}.get(args.workload)
     if fn is None:
@@ -871,6 +973,7 @@ def main():
     args = ap.parse_args()
     args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
                         "grover": "Grover iterations/s (26q FP64, marked index 42)",
+                        "hadamard": "gate-layers/s (H on every qubit, 30q FP64)",
                         "batched": "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
                         "served": SERVED_METRIC}.get(args.workload, args.workload)
     dist = Dist()
