@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}", "-ccbin", "g++"]
 
-ENGINE_SRCS = ["circuit.cpp", "planner.cpp", "engine.cpp", "kernels.cu", "batch.cu", "server.cpp"]
+ENGINE_SRCS = ["circuit.cpp", "planner.cpp", "engine.cpp", "kernels.cu", "batch.cu", "server.cpp", "hostcopy.cpp"]
 # Extra nvcc flags (e.g. -DHGM_MAXREG_F32=128) and an alternative output
 # folder, for building tuning variants side by side.
 EXTRA_FLAGS = os.environ.get("HGM_NVCC_EXTRA", "").split()

@@ -168,10 +168,7 @@ int hgm_state_upload(hgm_state *s, const void *host, int64_t bytes) {
     if (!st || !host) return fail(HGM_ERR_INVALID, "null argument");
     if (bytes != st->bytes()) return fail(HGM_ERR_INVALID, "upload of %lld bytes into a %lld-byte state",
                                           (long long)bytes, (long long)st->bytes());
-    cudaStream_t stream = (cudaStream_t)default_stream();
-    cudaError_t e = cudaMemcpyAsync(st->d, host, (size_t)bytes, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    return e == cudaSuccess ? HGM_OK : cuda_fail(e, "state upload");
+    return copy_state(st->d, host, (size_t)bytes, true, default_stream());
 }
 
 int hgm_state_download(const hgm_state *s, void *host, int64_t bytes) {
@@ -179,10 +176,7 @@ int hgm_state_download(const hgm_state *s, void *host, int64_t bytes) {
     if (!st || !host) return fail(HGM_ERR_INVALID, "null argument");
     if (bytes != st->bytes()) return fail(HGM_ERR_INVALID, "download of %lld bytes from a %lld-byte state",
                                           (long long)bytes, (long long)st->bytes());
-    cudaStream_t stream = (cudaStream_t)default_stream();
-    cudaError_t e = cudaMemcpyAsync(host, st->d, (size_t)bytes, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    return e == cudaSuccess ? HGM_OK : cuda_fail(e, "state download");
+    return copy_state(host, st->d, (size_t)bytes, false, default_stream());
 }
 
 int hgm_execute(hgm_state *s, const hgm_plan *p, int iterations, void *stream) {

@@ -150,6 +150,10 @@ struct Plan {
     ~Plan();
 };
 
+// Synchronous copy of a state between host and device memory (hostcopy.cpp):
+// large copies go through page-locked staging chunks on several threads.
+int copy_state(void *dst, const void *src, size_t bytes, bool to_device, void *stream);
+
 // force_small: plan the state for the one-CTA shared-memory path even when
 // it is large enough for the register tile (the batched kernel's small tasks).
 int build_plan(const std::vector<Op> &ops, int qubits, const hgm_plan_opts &opts, Plan *plan,

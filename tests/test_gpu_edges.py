@@ -134,3 +134,27 @@ def test_largest_states(sq, prec, n):
     idx, p = st.marginal_argmax((1 << 5) | 1)
     assert abs(p - 0.25) < 1e-6 and idx in (0, 1, 2, 3)
     st.free()
+
+
+@pytest.mark.parametrize("prec,n", [("f32", 25), ("f64", 26), ("f32", 28)])
+def test_staged_copy_round_trip(sq, prec, n):
+    """States of 256 MiB and more travel through page-locked staging chunks on
+    several host threads.  A chunk placed at the wrong offset would change the
+    per-bit probabilities the device computes; a byte lost on the way back
+    would break the exact round trip."""
+    rng = np.random.default_rng(n)
+    dt = np.complex64 if prec == "f32" else np.complex128
+    amp = np.empty(1 << n, dtype=dt)
+    amp.real = rng.random(1 << n)
+    amp.imag = np.arange(1 << n) / float(1 << n)     # index-dependent
+    st = sq.State(n, prec).upload(amp)
+    w = np.abs(amp.astype(np.complex128)) ** 2
+    total = w.sum()
+    assert abs(st.norm() - total) < 1e-6 * total
+    idx = np.arange(1 << n, dtype=np.int64)
+    for b in (0, 7, n - 5, n - 2, n - 1):
+        want = w[(idx >> b) & 1 == 1].sum()              # prob_one is not normalised
+        assert abs(st.prob_one(b) - want) < 1e-6 * total, b
+    back = st.download()
+    st.free()
+    assert np.array_equal(back.view(np.uint8), amp.view(np.uint8))
