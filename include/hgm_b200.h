@@ -109,6 +109,9 @@ int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t
  * laid out in simulador_quantico_b200/csrc/hgm_internal.h. */
 int hgm_plan_export(const hgm_plan *p, const void **passes, int64_t *n_passes, const void **phases,
                     int64_t *n_phases, const void **ops, int64_t *ops_bytes, int *warp_bits, int *small);
+/* The plan's register layouts (struct Lay: 16 int8 local tile bits per
+ * layout, thread bits first, then register bits), for the same emulation. */
+int hgm_plan_layouts(const hgm_plan *p, const int8_t **pos, int64_t *n_layouts);
 
 /* ---- device-resident states -------------------------------------------- */
 

@@ -115,6 +115,14 @@ int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t
     return HGM_OK;
 }
 
+int hgm_plan_layouts(const hgm_plan *p, const int8_t **pos, int64_t *n_layouts) {
+    const Plan *pl = reinterpret_cast<const Plan *>(p);
+    if (!pl) return fail(HGM_ERR_INVALID, "null plan");
+    if (pos) *pos = pl->layouts.empty() ? nullptr : pl->layouts[0].pos;
+    if (n_layouts) *n_layouts = (int64_t)pl->layouts.size();
+    return HGM_OK;
+}
+
 int hgm_plan_export(const hgm_plan *p, const void **passes, int64_t *n_passes, const void **phases,
                     int64_t *n_phases, const void **ops, int64_t *ops_bytes, int *warp_bits, int *small) {
     if (!p) return fail(HGM_ERR_INVALID, "null plan");

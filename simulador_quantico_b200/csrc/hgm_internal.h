@@ -49,8 +49,17 @@ struct Circuit {
 
 // ---- kernel-side encodings (shared with kernels.cuh) ----------------------
 
-// Register-phase layouts of a warp tile (see kernels.cuh).
-enum Layout : int32_t { LAYOUT_C = 0, LAYOUT_B = 1, LAYOUT_A = 2, LAYOUT_E = 3 };
+// Register layouts of a tile (kernels.cuh).  A layout gives every role of
+// a thread's view of the tile its local tile bit: thread bits t = 0..4+W
+// (lanes 0..4, then warps) at pos[t], register bits q = 0..R-1 at
+// pos[5 + W + q].  On the device a layout is a table of LAYOUT_HDR words
+// (byte offset in the transpose buffer of each register bit's unit step)
+// followed by one word per thread (byte offset of its register 0).
+constexpr int MAX_LAYOUT_ROLES = 16;
+constexpr int LAYOUT_HDR = 8;
+struct Lay {
+    int8_t pos[MAX_LAYOUT_ROLES];
+};
 
 enum DevKind : int32_t {
     K_DENSE = 0,   // general 2x2
@@ -96,26 +105,37 @@ struct alignas(16) DevOp {
 };
 
 struct DevPhase {
-    int32_t layout;
+    int32_t layout;          // index into the plan's layout table
     int32_t op_begin, op_end;
     int32_t xwarp;   // 1 if entering this phase needs a cross-warp transpose
 };
 
 constexpr int MAX_TILE_BITS = 16;
+// Runs of consecutive non-tile index bits: at most one more than tile bits.
+constexpr int MAX_FREE_RUNS = MAX_TILE_BITS + 2;
 
 struct PassArgs {
     int32_t n;            // qubits
     int32_t k;            // tile bits = 5 + R + W
     int32_t phase_begin, phase_end;
-    int32_t load_layout, store_layout;
+    int32_t load_layout, store_layout;  // layout table indices
     int32_t flags;        // PASS_* below
-    int32_t pad;
+    int32_t store_xwarp;  // the transpose into the store layout crosses warps
     int8_t tb[MAX_TILE_BITS];  // local tile bit -> global index bit
     uint64_t tile_mask;
     const DevPhase *phases;
     const void *ops;      // DevOp<Real>*
     double *norm_out;     // PASS_NORM: accumulate sum |a|^2 of stored amplitudes
     const double *scale_in; // PASS_SCALE: multiply loaded amplitudes by 1/sqrt(*scale_in)
+    const uint32_t *layouts;  // layout table, LAYOUT_HDR + 2^(5+W) words per layout
+    // The non-tile index bits as runs, lowest first: the tile number's next
+    // run_len[i] bits go to index bits run_pos[i] .. run_pos[i] + run_len[i] - 1.
+    int8_t run_pos[MAX_FREE_RUNS];
+    int8_t run_len[MAX_FREE_RUNS];
+    int32_t nruns;
+    // global index bit of every role of the load and store layouts
+    int8_t ld_gbit[MAX_LAYOUT_ROLES];
+    int8_t st_gbit[MAX_LAYOUT_ROLES];
 };
 
 constexpr int32_t PASS_NORM = 1;
@@ -139,11 +159,13 @@ struct Plan {
     bool small = false;               // n < 5 + reg_bits: single-CTA shared-memory path
     std::vector<PassArgs> passes;     // device pointers patched after upload
     std::vector<DevPhase> phases;
+    std::vector<Lay> layouts;         // every layout the phases use
     std::vector<unsigned char> ops_bytes;   // DevOp<Real>[] or SmallOp<Real>[]
     int64_t n_small_ops = 0;
     int64_t n_ops = 0, n_transposes = 0;
     // device copies
     void *d_phases = nullptr;
+    void *d_layouts = nullptr;
     void *d_ops = nullptr;
     int renorm_every = 0;
     double *d_norm = nullptr;         // renormalisation scratch (FP32 plans)

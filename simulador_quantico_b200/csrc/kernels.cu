@@ -141,12 +141,12 @@ static int setup_pass_kernel() {
 
 template <typename Real, int R, int W>
 static int launch_pass(void *state, const PassArgs &pa, cudaStream_t st) {
+    using A2 = typename V2<Real>::T;
     int rc = setup_pass_kernel<Real, R, W>();
     if (rc) return rc;
     const uint64_t tiles = 1ull << (pa.n - pa.k);
-    const int smem = tile_smem_elems<R, W>() * (int)sizeof(typename V2<Real>::T);
-    pass_kernel<Real, R, W><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<typename V2<Real>::T *>(state),
-                                                                    pa);
+    const int smem = tile_smem_elems<R, W>() * (int)sizeof(A2);
+    pass_kernel<Real, R, W><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<A2 *>(state), pa);
     count_launch();
     return HGM_OK;
 }
@@ -179,6 +179,7 @@ int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
     // every device pointer a launch passes must exist: an op list that was
     // never uploaded is refused here, not read through a null pointer
     if ((!p->ops_bytes.empty() && !p->d_ops) || (!p->phases.empty() && !p->d_phases) ||
+        (!p->layouts.empty() && !p->d_layouts) ||
         (p->renorm_every > 0 && !p->small && !p->d_norm))
         return fail(HGM_ERR_INVALID, "plan used before upload_plan");
     cudaStream_t st = pick(stream);
@@ -224,6 +225,7 @@ int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
 
 Plan::~Plan() {
     if (d_phases) cudaFree(d_phases);
+    if (d_layouts) cudaFree(d_layouts);
     if (d_ops) cudaFree(d_ops);
     if (d_norm) cudaFree(d_norm);
 }
@@ -244,12 +246,37 @@ int upload_plan(Plan *p) {
         if ((e = cudaMemcpy(p->d_phases, p->phases.data(), b, cudaMemcpyHostToDevice)) != cudaSuccess)
             return fail(HGM_ERR_CUDA, "plan phases copy: %s", cudaGetErrorString(e));
     }
+    if (!p->layouts.empty()) {
+        // per layout: the byte step of each register bit, then each thread's
+        // register-0 offset, in the padded transpose buffer (kernels.cuh)
+        const int R = p->reg_bits, W = p->warp_bits, nt = 32 << W;
+        const uint32_t esz = p->precision == HGM_F64 ? 16 : 8;
+        auto pad = [&](uint32_t j) { return (j + (j >> R)) * esz; };
+        std::vector<uint32_t> tab(p->layouts.size() * (LAYOUT_HDR + nt), 0u);
+        for (size_t l = 0; l < p->layouts.size(); l++) {
+            const Lay &lay = p->layouts[l];
+            uint32_t *e0 = tab.data() + l * (LAYOUT_HDR + nt);
+            for (int q = 0; q < R; q++) e0[q] = pad(1u << lay.pos[5 + W + q]);
+            for (int t = 0; t < nt; t++) {
+                uint32_t o = 0;
+                for (int b = 0; b < 5 + W; b++)
+                    if ((t >> b) & 1) o += pad(1u << lay.pos[b]);
+                e0[LAYOUT_HDR + t] = o;
+            }
+        }
+        const size_t b = tab.size() * sizeof(uint32_t);
+        if ((e = cudaMalloc(&p->d_layouts, b)) != cudaSuccess)
+            return fail(HGM_ERR_NOMEM, "plan layouts: %s", cudaGetErrorString(e));
+        if ((e = cudaMemcpy(p->d_layouts, tab.data(), b, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(HGM_ERR_CUDA, "plan layouts copy: %s", cudaGetErrorString(e));
+    }
     if (p->renorm_every > 0) {
         if ((e = cudaMalloc(&p->d_norm, 64 * sizeof(double))) != cudaSuccess)
             return fail(HGM_ERR_NOMEM, "plan norm slots: %s", cudaGetErrorString(e));
     }
     for (PassArgs &pa : p->passes) {
         pa.phases = reinterpret_cast<const DevPhase *>(p->d_phases);
+        pa.layouts = reinterpret_cast<const uint32_t *>(p->d_layouts);
         pa.ops = p->d_ops;
     }
     return HGM_OK;

@@ -7,24 +7,17 @@
 // holds 2^(5+R) and the CTA 2^W warps.  The tile is the set of state
 // indices that agree on every index bit outside the pass's K tile bits;
 // local tile bit q is index bit tb[q].  Which local bits are the lane,
-// register and warp bits of a thread is fixed by one of four layouts:
-//
-//   C: lanes = local 0..4,   regs = local 5..4+R,  warps = local 5+R..
-//   B: regs  = local 0..R-1, lanes = local R..R+4, warps = local 5+R..
-//   E: (R = 4 only) lanes = local 0..3 and 8, regs = local 4..7, warps 9..
-//   A: lanes = local 0..4,   warps = local 5..4+W, regs = local 5+W..4+W+R
+// warp and register bits of a thread is the current phase's layout, a table
+// the planner builds (struct Lay): any R local bits can be the register bits.
 //
 // A gate whose target is a register bit of the current layout is applied
 // entirely in registers.  Switching layout is a transpose through shared
-// memory: C, B and E keep the warp bits in place, so switching among them
-// stays inside each warp (__syncwarp); anything with A crosses warps
-// (__syncthreads).  Layouts C and A put the lanes on local bits 0..4, whose
-// low `low_bits` bits are the lowest index bits of the state: global loads
-// and stores are issued in those layouts and each warp instruction moves
-// whole 128-byte runs.  Shared memory is XOR-swizzled,
-// phys(j) = j ^ ((j >> R) & S), S = 7 for 16-byte FP64 amplitudes (a quarter
-// warp per shared-memory wavefront) and 15 for 8-byte FP32 amplitudes (a
-// half warp), which keeps every layout's accesses free of bank conflicts.
+// memory; when both layouts keep the warp bits in place it stays inside
+// each warp (__syncwarp), otherwise it crosses warps (__syncthreads).  The
+// load and store layouts put thread bits 0..low_bits-1 on the lowest index
+// bits of the state, so each warp instruction moves whole 128-byte runs.
+// Shared memory is padded (pad_slot below); the planner only builds layouts
+// whose accesses are free of bank conflicts under that padding.
 //
 // State loads and stores bypass L1 (ld/st .cg): every amplitude is touched
 // once per pass, and a tile written by one CTA may be read by another CTA of
@@ -84,43 +77,25 @@ __device__ __forceinline__ uint32_t pad_slot(uint32_t j) {
     return j + (j >> R);
 }
 
-// Slot step between consecutive register labels of a layout: its register
-// bits start at local bit s, and pad_slot(l << s) = l * (2^s + 2^(s-R)).
-template <int R, int W, int LAY>
-__host__ __device__ constexpr uint32_t reg_slot_stride() {
-    constexpr int s = LAY == LAYOUT_C ? 5 : LAY == LAYOUT_B ? 0 : LAY == LAYOUT_E ? 4 : 5 + W;
-    return (1u << s) + (s >= R ? (1u << (s - R)) : 0u);
-}
-
 // Shared memory of one tile's transposes, in amplitudes.
 template <int R, int W>
 __host__ __device__ constexpr int tile_smem_elems() {
     return (1 << (5 + R + W)) + (1 << (5 + W));
 }
 
-template <int R, int W, int LAY>
-__device__ __forceinline__ uint32_t local_index(uint32_t lane, uint32_t warp, uint32_t r) {
-    if (LAY == LAYOUT_C) return lane | (r << 5) | (warp << (5 + R));
-    if (LAY == LAYOUT_B) return r | (lane << R) | (warp << (5 + R));
-    if (LAY == LAYOUT_E) return (lane & 15u) | (r << 4) | ((lane >> 4) << 8) | (warp << 9);
-    return lane | (warp << 5) | (r << (5 + W));
-}
-
 // Offset (in amplitudes) of a thread's register-0 amplitude and the R
-// register-bit strides, for a global-capable layout (C or A).  The layout is
-// a template argument so every tile-bit lookup uses a constant index into the
-// kernel parameters (a runtime index would copy them to local memory).
-template <int R, int W, int LAY>
-__device__ __forceinline__ void thread_geometry(const PassArgs &pa, uint32_t lane, uint32_t warp, uint64_t &off,
+// register-bit strides in the state, for a layout given by the global index
+// bit of each role (thread bits 0..4+W, then register bits).  Every lookup
+// uses a constant index into the kernel parameters (a runtime index would
+// copy them to local memory).
+template <int R, int W>
+__device__ __forceinline__ void thread_geometry(const int8_t (&gb)[MAX_LAYOUT_ROLES], uint32_t thr, uint64_t &off,
                                                 uint64_t (&rs)[R]) {
-    constexpr int ws = (LAY == LAYOUT_A) ? 5 : 5 + R, rsb = (LAY == LAYOUT_A) ? 5 + W : 5;
     off = 0;
 #pragma unroll
-    for (int q = 0; q < 5; q++) off |= (uint64_t)((lane >> q) & 1) << pa.tb[q];
+    for (int t = 0; t < 5 + W; t++) off |= (uint64_t)((thr >> t) & 1) << gb[t];
 #pragma unroll
-    for (int q = 0; q < W; q++) off |= (uint64_t)((warp >> q) & 1) << pa.tb[ws + q];
-#pragma unroll
-    for (int q = 0; q < R; q++) rs[q] = (uint64_t)1 << pa.tb[rsb + q];
+    for (int q = 0; q < R; q++) rs[q] = (uint64_t)1 << gb[5 + W + q];
 }
 
 template <int R, int r>
@@ -673,89 +648,85 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
 
 // ---- layout transposes through shared memory --------------------------------
 
-template <typename Real, typename A2, int R, int W, int FROM, int TO>
-__device__ __forceinline__ void transpose_t(A2 (&a)[1 << R], A2 *sm, uint32_t lane, uint32_t warp,
-                                            bool sync_cta_before, bool cross, uint32_t xr) {
+// Moves the registers from layout `from` to layout `to` (layout tables: the
+// byte offset of each register bit's unit step, then each thread's register-0
+// offset).  Register r holds label r ^ xr (apply_op): its slot is the
+// thread's base plus the steps of the bits of r ^ xr, i.e. the base moved by
+// the steps of xr plus the steps of r with those bits negated.
+template <typename A2, int R>
+__device__ __forceinline__ void transpose(A2 (&a)[1 << R], unsigned char *sm, uint32_t thr,
+                                          const uint32_t *__restrict__ from, const uint32_t *__restrict__ to,
+                                          bool sync_cta_before, bool cross, uint32_t xr) {
+    uint32_t wb = __ldg(from + LAYOUT_HDR + thr), s[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) s[q] = __ldg(from + q);
     if (sync_cta_before) __syncthreads();
     else __syncwarp();
-    // register r holds label r ^ xr
-    constexpr uint32_t sf = reg_slot_stride<R, W, FROM>(), st = reg_slot_stride<R, W, TO>();
-    A2 *w = sm + pad_slot<R>(local_index<R, W, FROM>(lane, warp, 0));
-    if (xr == 0) {
 #pragma unroll
-        for (int r = 0; r < (1 << R); r++) w[sf * r] = a[r];
-    } else {
-#pragma unroll
-        for (int r = 0; r < (1 << R); r++) w[sf * (r ^ xr)] = a[r];
+    for (int q = 0; q < R; q++) {
+        const bool f = (xr >> q) & 1u;
+        wb += f ? s[q] : 0u;
+        s[q] = f ? 0u - s[q] : s[q];
     }
+#pragma unroll
+    for (int r = 0; r < (1 << R); r++) {
+        uint32_t o = wb;
+#pragma unroll
+        for (int q = 0; q < R; q++)
+            if (r & (1 << q)) o += s[q];
+        *reinterpret_cast<A2 *>(sm + o) = a[r];
+    }
+    uint32_t rb = __ldg(to + LAYOUT_HDR + thr), u[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) u[q] = __ldg(to + q);
     if (cross) __syncthreads();
     else __syncwarp();
-    const A2 *rd = sm + pad_slot<R>(local_index<R, W, TO>(lane, warp, 0));
 #pragma unroll
-    for (int r = 0; r < (1 << R); r++) a[r] = rd[st * r];
-}
-
-template <typename Real, typename A2, int R, int W, int FROM>
-__device__ __forceinline__ void transpose_from(int to, A2 (&a)[1 << R], A2 *sm, uint32_t lane, uint32_t warp,
-                                               bool sync_cta_before, bool cross, uint32_t xr) {
-    switch (to) {
-        case LAYOUT_C: transpose_t<Real, A2, R, W, FROM, LAYOUT_C>(a, sm, lane, warp, sync_cta_before, cross, xr); break;
-        case LAYOUT_B: transpose_t<Real, A2, R, W, FROM, LAYOUT_B>(a, sm, lane, warp, sync_cta_before, cross, xr); break;
-        case LAYOUT_E:
-            if (R == 4) transpose_t<Real, A2, R, W, FROM, LAYOUT_E>(a, sm, lane, warp, sync_cta_before, cross, xr);
-            break;
-        default: transpose_t<Real, A2, R, W, FROM, LAYOUT_A>(a, sm, lane, warp, sync_cta_before, cross, xr); break;
+    for (int r = 0; r < (1 << R); r++) {
+        uint32_t o = rb;
+#pragma unroll
+        for (int q = 0; q < R; q++)
+            if (r & (1 << q)) o += u[q];
+        a[r] = *reinterpret_cast<const A2 *>(sm + o);
     }
 }
 
-template <typename Real, typename A2, int R, int W>
-__device__ __forceinline__ void transpose(int from, int to, A2 (&a)[1 << R], A2 *sm, uint32_t lane, uint32_t warp,
-                                          bool sync_cta_before, bool cross, uint32_t xr) {
-    switch (from) {
-        case LAYOUT_C: transpose_from<Real, A2, R, W, LAYOUT_C>(to, a, sm, lane, warp, sync_cta_before, cross, xr); break;
-        case LAYOUT_B: transpose_from<Real, A2, R, W, LAYOUT_B>(to, a, sm, lane, warp, sync_cta_before, cross, xr); break;
-        case LAYOUT_E:
-            if (R == 4) transpose_from<Real, A2, R, W, LAYOUT_E>(to, a, sm, lane, warp, sync_cta_before, cross, xr);
-            break;
-        default: transpose_from<Real, A2, R, W, LAYOUT_A>(to, a, sm, lane, warp, sync_cta_before, cross, xr); break;
-    }
-}
-
-// Index of tile `t`: deposit the bits of t into the non-tile index bits.
-__device__ __forceinline__ uint64_t tile_base(uint64_t t, uint64_t tile_mask, int n) {
-    uint64_t free_bits = ~tile_mask & ((n >= 64) ? ~0ull : ((1ull << n) - 1));
+// Index of tile `t`: deposit the bits of t into the non-tile index bits, one
+// run of consecutive non-tile bits at a time (uniform across the CTA).
+__device__ __forceinline__ uint64_t tile_base(uint64_t t, const PassArgs &pa) {
     uint64_t base = 0;
-    while (free_bits) {
-        const int g = __ffsll((long long)free_bits) - 1;
-        free_bits &= free_bits - 1;
-        base |= (t & 1ull) << g;
-        t >>= 1;
+#pragma unroll
+    for (int i = 0; i < MAX_FREE_RUNS; i++) {
+        if (i >= pa.nruns) break;
+        const int len = pa.run_len[i];
+        base |= (t & ((1ull << len) - 1ull)) << pa.run_pos[i];
+        t >>= len;
     }
     return base;
 }
 
-template <typename Real, int R, int W, int LAY>
+template <typename Real, int R, int W>
 __device__ __forceinline__ void load_tile(typename V2<Real>::T (&a)[1 << R],
                                           const typename V2<Real>::T *__restrict__ state, const PassArgs &pa,
-                                          uint64_t base, uint32_t lane, uint32_t warp) {
+                                          uint64_t base, uint32_t thr) {
     using A2 = typename V2<Real>::T;
     uint64_t off, rs[R];
-    thread_geometry<R, W, LAY>(pa, lane, warp, off, rs);
+    thread_geometry<R, W>(pa.ld_gbit, thr, off, rs);
     LoadF<A2, R> f{a, state + (base | off), rs};
     Unroll<1 << R>::run(f);
 }
 
-template <typename Real, int R, int W, int LAY>
+template <typename Real, int R, int W>
 __device__ __forceinline__ void store_tile(const typename V2<Real>::T (&a)[1 << R],
                                            typename V2<Real>::T *__restrict__ state, const PassArgs &pa,
-                                           uint64_t base, uint32_t warp, uint32_t xr) {
+                                           uint64_t base, uint32_t xr) {
     using A2 = typename V2<Real>::T;
-    // The lane index is re-read so the store geometry is recomputed here
+    // The thread index is re-read so the store geometry is recomputed here
     // instead of being held in registers through every phase.
-    uint32_t lane;
-    asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
+    uint32_t thr;
+    asm volatile("mov.u32 %0, %%tid.x;" : "=r"(thr));
     uint64_t off, rs[R];
-    thread_geometry<R, W, LAY>(pa, lane, warp, off, rs);
+    thread_geometry<R, W>(pa.st_gbit, thr, off, rs);
     uint64_t xo = 0;
 #pragma unroll
     for (int q = 0; q < R; q++)
@@ -764,21 +735,20 @@ __device__ __forceinline__ void store_tile(const typename V2<Real>::T (&a)[1 << 
     Unroll<1 << R>::run(f);
 }
 
-// Runs one pass over tile `tile`.  Shared by the plain pass kernel and the
-// batched persistent kernel.
+// Applies a pass's phases to a tile already in registers (loaded in the
+// pass's load layout) and stores it.  `prev_cross`: the CTA's previous use
+// of `sm` may still be read by other warps, so the first transpose must
+// synchronise the CTA before writing.
 template <typename Real, int R, int W>
-__device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ state, const PassArgs &pa, uint64_t tile,
-                                         typename V2<Real>::T *sm) {
+__device__ __forceinline__ void finish_tile(typename V2<Real>::T (&a)[1 << R], typename V2<Real>::T *__restrict__ state,
+                                            const PassArgs &pa, uint64_t base, typename V2<Real>::T *sm,
+                                            bool prev_cross) {
     using A2 = typename V2<Real>::T;
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t thr = lane | (warp << 5);
-    const uint64_t base = tile_base(tile, pa.tile_mask, pa.n);
+    constexpr uint32_t LS = LAYOUT_HDR + (32u << W);  // words per layout table
+    const uint32_t thr = threadIdx.x, lane = thr & 31;
     const DevOp<Real> *__restrict__ ops = reinterpret_cast<const DevOp<Real> *>(pa.ops);
-
-    A2 a[1 << R];
+    unsigned char *smb = reinterpret_cast<unsigned char *>(sm);
     int cur = pa.load_layout;
-    if (cur == LAYOUT_A) load_tile<Real, R, W, LAYOUT_A>(a, state, pa, base, lane, warp);
-    else load_tile<Real, R, W, LAYOUT_C>(a, state, pa, base, lane, warp);
     if (pa.flags & PASS_SCALE) {
         const Real s = (Real)rsqrt(*pa.scale_in);
 #pragma unroll
@@ -787,12 +757,12 @@ __device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ stat
             a[r].y *= s;
         }
     }
-    bool prev_cross = false;
     uint32_t xr = 0;  // register relabeling (apply_op)
     for (int p = pa.phase_begin; p < pa.phase_end; p++) {
         const DevPhase ph = pa.phases[p];
         if (ph.layout != cur) {
-            transpose<Real, A2, R, W>(cur, ph.layout, a, sm, lane, warp, prev_cross || ph.xwarp, ph.xwarp != 0, xr);
+            transpose<A2, R>(a, smb, thr, pa.layouts + cur * LS, pa.layouts + ph.layout * LS, prev_cross || ph.xwarp,
+                             ph.xwarp != 0, xr);
             xr = 0;
             prev_cross = ph.xwarp != 0;
             cur = ph.layout;
@@ -806,13 +776,11 @@ __device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ stat
         }
     }
     if (cur != pa.store_layout) {
-        const bool cross = (cur == LAYOUT_A) != (pa.store_layout == LAYOUT_A);
-        transpose<Real, A2, R, W>(cur, pa.store_layout, a, sm, lane, warp, prev_cross || cross, cross, xr);
+        transpose<A2, R>(a, smb, thr, pa.layouts + cur * LS, pa.layouts + pa.store_layout * LS,
+                         prev_cross || pa.store_xwarp, pa.store_xwarp != 0, xr);
         xr = 0;
-        cur = pa.store_layout;
     }
-    if (cur == LAYOUT_A) store_tile<Real, R, W, LAYOUT_A>(a, state, pa, base, warp, xr);
-    else store_tile<Real, R, W, LAYOUT_C>(a, state, pa, base, warp, xr);
+    store_tile<Real, R, W>(a, state, pa, base, xr);
     if (pa.flags & PASS_NORM) {
         double acc = 0.0;
 #pragma unroll
@@ -821,6 +789,18 @@ __device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ stat
         for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) atomicAdd(pa.norm_out, acc);
     }
+}
+
+// Runs one pass over tile `tile`.  Shared by the plain pass kernel and the
+// batched persistent kernel.
+template <typename Real, int R, int W>
+__device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ state, const PassArgs &pa, uint64_t tile,
+                                         typename V2<Real>::T *sm) {
+    using A2 = typename V2<Real>::T;
+    const uint64_t base = tile_base(tile, pa);
+    A2 a[1 << R];
+    load_tile<Real, R, W>(a, state, pa, base, threadIdx.x);
+    finish_tile<Real, R, W>(a, state, pa, base, sm, false);
 }
 
 }  // namespace hgm

@@ -15,8 +15,8 @@
 //   * optionally fuses adjacent gates on the same target and controls into
 //     one matrix (product formed in FP64).
 // Inside a pass, gates are split into register phases of the register-tile
-// kernel (kernels.cuh): each phase holds the gates whose targets are
-// register bits of one of its layouts (C, B, A and, for FP64 tiles, E).
+// kernel (kernels.cuh): each phase holds gates whose targets are register
+// bits of its layout, a choice of R of the tile's local bits.
 #include <algorithm>
 #include <cstring>
 
@@ -93,43 +93,107 @@ std::vector<SOp> fuse_ops(const std::vector<Op> &ops, bool fuse) {
     return out;
 }
 
-// Role of local tile bit q in a layout of the register tile (kernels.cuh):
-//   C: lanes = local 0..4,   regs = local 5..4+R,  warps = local 5+R..
-//   B: regs  = local 0..R-1, lanes = local R..R+4, warps = local 5+R..
-//   E: (R = 4) lanes = local 0..3 and 8, regs = local 4..7, warps = local 9..
-//   A: lanes = local 0..4,   warps = local 5..4+W, regs = local 5+W..4+W+R
-enum RoleKind { ROLE_LANE = 0, ROLE_REG = 1, ROLE_WARP = 2 };
+// Role of each local tile bit in a layout (struct Lay): thread bit t (lanes
+// 0..4, warps 5..) or register bit q.
+enum RoleKind { ROLE_THREAD = 0, ROLE_REG = 1 };
 struct Role {
     int kind, idx;
 };
-Role role(int layout, int R, int W, int q) {
-    switch (layout) {
-        case LAYOUT_C:
-            if (q < 5) return {ROLE_LANE, q};
-            if (q < 5 + R) return {ROLE_REG, q - 5};
-            return {ROLE_WARP, q - 5 - R};
-        case LAYOUT_B:
-            if (q < R) return {ROLE_REG, q};
-            if (q < R + 5) return {ROLE_LANE, q - R};
-            return {ROLE_WARP, q - 5 - R};
-        case LAYOUT_E:
-            if (q < 4) return {ROLE_LANE, q};
-            if (q < 8) return {ROLE_REG, q - 4};
-            if (q == 8) return {ROLE_LANE, 4};
-            return {ROLE_WARP, q - 9};
-        default:
-            if (q < 5) return {ROLE_LANE, q};
-            if (q < 5 + W) return {ROLE_WARP, q - 5};
-            return {ROLE_REG, q - 5 - W};
+struct Roles {
+    Role of[MAX_LAYOUT_ROLES];
+    Roles(const Lay &lay, int R, int W) {
+        for (int k = 0; k < MAX_LAYOUT_ROLES; k++) of[k] = {ROLE_THREAD, -1};
+        for (int k = 0; k < 5 + W + R; k++)
+            of[lay.pos[k]] = k < 5 + W ? Role{ROLE_THREAD, k} : Role{ROLE_REG, k - 5 - W};
     }
-}
-inline bool in_regs(int layout, int R, int W, int loc) { return role(layout, R, W, loc).kind == ROLE_REG; }
+};
+
+// Builds layouts.  Every layout keeps a warp's shared-memory accesses free of
+// bank conflicts: with slot(j) = j + (j >> R) (kernels.cuh pad_slot), the
+// unit slot of local bit q is 1, 2, 4, 8 (mod 8 for 16-byte, mod 16 for
+// 8-byte amplitudes) exactly for q = i or q = i + R, i < NB, where NB = 3
+// (FP64: a quarter warp per 128-byte wavefront) or 4 (FP32: a half warp).
+// So thread bit i < NB sits on local bit i, or on i + R when i is a register
+// bit, and no layout takes both i and i + R as register bits.  A layout is
+// "coalesced" when thread bits 0..L-1 are local bits 0..L-1, the low index
+// bits: only such layouts load and store the state.
+struct LayoutMaker {
+    int R, W, K, NB, L;
+    bool feasible(uint32_t S) const {
+        if (__builtin_popcount(S) > R) return false;
+        for (int i = 0; i < NB; i++)
+            if (((S >> i) & 1) && ((S >> (i + R)) & 1)) return false;
+        return true;
+    }
+    bool coalesced(const Lay &lay) const {
+        for (int i = 0; i < L && i < 5; i++)
+            if (lay.pos[i] != i) return false;
+        return true;
+    }
+    // Register bits S (R of them, feasible); warp bits where `prev` has them
+    // when those local bits are free, so that the transpose stays inside
+    // each warp.
+    Lay make(uint32_t S, const Lay *prev) const {
+        Lay lay;
+        for (int k = 0; k < MAX_LAYOUT_ROLES; k++) lay.pos[k] = -1;
+        uint32_t used = S;
+        int k = 5 + W;
+        for (int q = 0; q < K; q++)
+            if ((S >> q) & 1) lay.pos[k++] = (int8_t)q;
+        for (int i = 0; i < NB; i++) {
+            const int q = ((S >> i) & 1) ? i + R : i;
+            lay.pos[i] = (int8_t)q;
+            used |= 1u << q;
+        }
+        for (int i = NB; i < L && i < 5; i++)
+            if (!((used >> i) & 1)) {
+                lay.pos[i] = (int8_t)i;
+                used |= 1u << i;
+            }
+        if (prev)
+            for (int w = 0; w < W; w++) {
+                const int q = prev->pos[5 + w];
+                if (!((used >> q) & 1)) {
+                    lay.pos[5 + w] = (int8_t)q;
+                    used |= 1u << q;
+                }
+            }
+        int q = 0;
+        for (int t = 0; t < 5 + W; t++) {
+            if (lay.pos[t] >= 0) continue;
+            while ((used >> q) & 1) q++;
+            lay.pos[t] = (int8_t)q;
+            used |= 1u << q;
+        }
+        return lay;
+    }
+    // Adds bits to S until it has R: `first` in order, then bits at or above
+    // L, then any, each only if S stays feasible.
+    uint32_t fill(uint32_t S, uint32_t first) const {
+        for (int pass = 0; pass < 3 && __builtin_popcount(S) < R; pass++) {
+            for (int q = 0; q < K && __builtin_popcount(S) < R; q++) {
+                const bool want = pass == 0 ? ((first >> q) & 1) : pass == 1 ? q >= L : true;
+                if (want && !((S >> q) & 1) && feasible(S | (1u << q))) S |= 1u << q;
+            }
+        }
+        return S;
+    }
+    static uint32_t regs(const Lay &lay, int R, int W) {
+        uint32_t S = 0;
+        for (int q = 0; q < R; q++) S |= 1u << lay.pos[5 + W + q];
+        return S;
+    }
+    bool same_warps(const Lay &a, const Lay &b) const {
+        for (int w = 0; w < W; w++)
+            if (a.pos[5 + w] != b.pos[5 + w]) return false;
+        return true;
+    }
+};
 
 template <typename Real>
-DevOp<Real> encode(const SOp &o, int layout, int R, int W, const int loc_of[64], uint64_t tile_mask) {
+DevOp<Real> encode(const SOp &o, const Roles &ro, const int loc_of[64], uint64_t tile_mask) {
     DevOp<Real> d;
     memset(&d, 0, sizeof d);
-    auto thr_index = [&](const Role &rl) -> int { return rl.kind == ROLE_LANE ? rl.idx : 5 + rl.idx; };
     uint64_t cm = o.cmask;
     while (cm) {
         int g = __builtin_ctzll(cm);
@@ -140,14 +204,13 @@ DevOp<Real> encode(const SOp &o, int layout, int R, int W, const int loc_of[64],
             d.cv_glob |= uint64_t(v) << g;
             continue;
         }
-        Role rl = role(layout, R, W, loc_of[g]);
+        const Role rl = ro.of[loc_of[g]];
         if (rl.kind == ROLE_REG) {
             d.cm_reg |= 1u << rl.idx;
             d.cv_reg |= v << rl.idx;
         } else {
-            int t = thr_index(rl);
-            d.cm_thr |= 1u << t;
-            d.cv_thr |= v << t;
+            d.cm_thr |= 1u << rl.idx;
+            d.cv_thr |= v << rl.idx;
         }
     }
     const cplx *m = o.m;
@@ -161,8 +224,8 @@ DevOp<Real> encode(const SOp &o, int layout, int R, int W, const int loc_of[64],
     if (!((tile_mask >> g) & 1)) {
         d.tpos = TPOS_GLOBAL + g;  // diagonal gates only
     } else {
-        Role rl = role(layout, R, W, loc_of[g]);
-        d.tpos = rl.kind == ROLE_REG ? rl.idx : TPOS_THREAD + thr_index(rl);
+        const Role rl = ro.of[loc_of[g]];
+        d.tpos = rl.kind == ROLE_REG ? rl.idx : TPOS_THREAD + rl.idx;
     }
     for (int k = 0; k < 4; k++) {
         d.m[2 * k] = (Real)m[k].real();
@@ -176,7 +239,7 @@ DevOp<Real> encode(const SOp &o, int layout, int R, int W, const int loc_of[64],
 // factors (kernels.cuh apply_phase_block).  Returns false when fewer than
 // `min_terms` qualify.
 template <typename Real>
-bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, int layout, int R, int W,
+bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const Roles &ro, int R,
                       const int loc_of[64], uint64_t tmask, int min_terms, std::vector<DevOp<Real>> &out) {
     // category lists: 0 = F, 1 + b = G[b], 1 + R + b = H[b], 1 + 2R + b = D[b]
     std::vector<std::vector<int>> cat(1 + 3 * R);
@@ -186,7 +249,7 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, int l
     uint64_t bn = 0, bd = 0;
     auto loc_role = [&](int g, Role &rl) -> bool {  // false: not a tile bit
         if (!((tmask >> g) & 1)) return false;
-        rl = role(layout, R, W, loc_of[g]);
+        rl = ro.of[loc_of[g]];
         return true;
     };
     for (int idx : rest) {
@@ -242,10 +305,10 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, int l
     memcpy(head.m, counts, 16);
     out.push_back(head);
     // records in the kernel's walk order: F, then per register bit b: G[b], H[b], D[b]
-    for (int idx : cat[0]) out.push_back(encode<Real>(ops[idx], layout, R, W, loc_of, tmask));
+    for (int idx : cat[0]) out.push_back(encode<Real>(ops[idx], ro, loc_of, tmask));
     for (int b = 0; b < R; b++)
         for (int k : {1 + b, 1 + R + b, 1 + 2 * R + b})
-            for (int idx : cat[k]) out.push_back(encode<Real>(ops[idx], layout, R, W, loc_of, tmask));
+            for (int idx : cat[k]) out.push_back(encode<Real>(ops[idx], ro, loc_of, tmask));
     for (int q = 0; q < table_recs; q++) {
         DevOp<Real> rec;
         memset(&rec, 0, sizeof rec);
@@ -270,11 +333,11 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, int l
 // register bit first) -- if there are at least two; else a phase block of
 // two; else a layer of one; else the first remaining gate on its own record.
 template <typename Real>
-void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, int R, int W, const int loc_of[64],
+void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, const Roles &ro, int R, const int loc_of[64],
                 uint64_t tmask, std::vector<DevOp<Real>> &out) {
     std::vector<int> keep;
     while (!rest.empty()) {
-        if (emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 3, out)) continue;
+        if (emit_phase_block<Real>(ops, rest, ro, R, loc_of, tmask, 3, out)) continue;
         int slot[8];
         for (int k = 0; k < 8; k++) slot[k] = -1;
         int found = 0;
@@ -284,7 +347,7 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, 
             const SOp &op = ops[idx];
             bool cand = false;
             if (op.mc == MC_DENSE && op.cmask == 0 && !conflicts(op, bn, bd)) {
-                Role rl = role(layout, R, W, loc_of[op.target]);
+                const Role rl = ro.of[loc_of[op.target]];
                 if (rl.kind == ROLE_REG && slot[rl.idx] < 0) {
                     slot[rl.idx] = idx;
                     found++;
@@ -305,7 +368,7 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, 
         // that a wider layer can still form behind it
         bool lone = false;
         if (found == 1) {
-            if (emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 2, out)) continue;
+            if (emit_phase_block<Real>(ops, rest, ro, R, loc_of, tmask, 2, out)) continue;
             for (int k = 0; k < R; k++) lone = lone || slot[k] == rest[0];
         }
         if (found >= 2 || lone) {
@@ -317,16 +380,16 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, int layout, 
                 if (slot[k] >= 0) head.cm_reg |= 1u << k;
             out.push_back(head);
             for (int k = 0; k < R; k++)
-                if (slot[k] >= 0) out.push_back(encode<Real>(ops[slot[k]], layout, R, W, loc_of, tmask));
+                if (slot[k] >= 0) out.push_back(encode<Real>(ops[slot[k]], ro, loc_of, tmask));
             for (int idx : rest) {
                 bool member = false;
                 for (int k = 0; k < R; k++) member = member || slot[k] == idx;
                 if (!member) keep.push_back(idx);
             }
-        } else if (found != 1 && emit_phase_block<Real>(ops, rest, layout, R, W, loc_of, tmask, 2, out)) {
+        } else if (found != 1 && emit_phase_block<Real>(ops, rest, ro, R, loc_of, tmask, 2, out)) {
             continue;
         } else {
-            out.push_back(encode<Real>(ops[rest[0]], layout, R, W, loc_of, tmask));
+            out.push_back(encode<Real>(ops[rest[0]], ro, loc_of, tmask));
             keep.assign(rest.begin() + 1, rest.end());
         }
         rest.swap(keep);
@@ -376,6 +439,13 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
     const uint64_t all_bits = (n >= 64) ? ~uint64_t(0) : ((uint64_t(1) << n) - 1);
     std::vector<DevOp<Real>> dev_ops;
     dev_ops.reserve(ops.size());
+    const LayoutMaker lm{R, W, K, R == 4 ? 3 : 4, L};
+    auto intern = [&](const Lay &lay) {
+        for (size_t i = 0; i < plan->layouts.size(); i++)
+            if (!memcmp(plan->layouts[i].pos, lay.pos, sizeof lay.pos)) return (int)i;
+        plan->layouts.push_back(lay);
+        return (int)plan->layouts.size() - 1;
+    };
 
     OpList list((int)ops.size());
     std::vector<int> pass_ops;
@@ -419,8 +489,8 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
                 tcount++;
             }
         }
-        // local positions: low bits fixed, then by first dense use into
-        // C-register slots, A-only slots, then B-only (lane) slots.
+        // local positions: the low bits at local 0..L-1; the others by first
+        // dense use at local 5 and up, then the lane bits above L
         std::vector<int> order;
         uint64_t placed = (uint64_t(1) << L) - 1;
         for (int idx : pass_ops) {
@@ -436,7 +506,6 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
                 placed |= uint64_t(1) << g;
                 order.push_back(g);
             }
-        // register slots of C, then those only A reaches, then E's, then B's
         std::vector<int> slots;
         for (int q = 5; q < 5 + R; q++) slots.push_back(q);
         for (int q = 5 + R; q < 5 + R + W; q++) slots.push_back(q);
@@ -457,66 +526,120 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
             pa.tb[slots[j]] = (int8_t)order[j];
         }
         pa.tile_mask = tmask;
+        for (int g = 0; g < n;) {
+            if ((tmask >> g) & 1) {
+                g++;
+                continue;
+            }
+            int e = g;
+            while (e < n && !((tmask >> e) & 1)) e++;
+            pa.run_pos[pa.nruns] = (int8_t)g;
+            pa.run_len[pa.nruns] = (int8_t)(e - g);
+            pa.nruns++;
+            g = e;
+        }
 
-        // register phases
+        // register phases: each takes the gates that can move to the front
+        // with their targets on its register bits.  A phase keeps the
+        // previous layout unless a new register set, chosen first-fit from
+        // the pending gates, takes more of them.
         pa.phase_begin = (int)plan->phases.size();
         std::vector<int> pending = pass_ops;
         int cur = -1;
-        const int layouts[4] = {LAYOUT_C, LAYOUT_A, LAYOUT_E, LAYOUT_B};
         std::vector<int> taken, rest;
-        while (!pending.empty()) {
-            int best = -1, best_count = -1;
-            for (int li = 0; li < 4; li++) {
-                int lay = layouts[li];
-                if (lay == LAYOUT_A && W == 0) continue;
-                if (lay == LAYOUT_E && R != 4) continue;
-                uint64_t bn = 0, bd = 0;
-                int count = 0;
-                for (int idx : pending) {
-                    const SOp &op = ops[idx];
-                    bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(lay, R, W, loc_of[op.target]));
-                    if (ok) count++;
-                    else {
-                        bn |= op.nd();
-                        bd |= op.dg();
-                    }
-                }
-                if (count > best_count || (count == best_count && lay == cur)) {
-                    best = lay;
-                    best_count = count;
-                }
-            }
-            taken.clear();
-            rest.clear();
+        auto walk = [&](uint32_t S, std::vector<int> *tk, std::vector<int> *rs) {
             uint64_t bn = 0, bd = 0;
+            int count = 0;
             for (int idx : pending) {
                 const SOp &op = ops[idx];
-                bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || in_regs(best, R, W, loc_of[op.target]));
-                if (ok) taken.push_back(idx);
-                else {
-                    rest.push_back(idx);
+                bool ok = !conflicts(op, bn, bd) && (op.mc == MC_DIAG || ((S >> loc_of[op.target]) & 1));
+                if (ok) {
+                    count++;
+                    if (tk) tk->push_back(idx);
+                } else {
+                    if (rs) rs->push_back(idx);
                     bn |= op.nd();
                     bd |= op.dg();
                 }
             }
+            return count;
+        };
+        auto first_fit = [&](uint32_t prefer) {
+            uint32_t S = 0;
+            uint64_t bn = 0, bd = 0;
+            for (int idx : pending) {
+                const SOp &op = ops[idx];
+                bool ok = !conflicts(op, bn, bd);
+                if (ok && op.mc != MC_DIAG) {
+                    const uint32_t b = 1u << loc_of[op.target];
+                    if (!(S & b)) {
+                        if (__builtin_popcount(S) < R && lm.feasible(S | b)) S |= b;
+                        else ok = false;
+                    }
+                }
+                if (!ok) {
+                    bn |= op.nd();
+                    bd |= op.dg();
+                }
+            }
+            return lm.fill(S, prefer);
+        };
+        while (!pending.empty()) {
+            const uint32_t cur_S = cur >= 0 ? LayoutMaker::regs(plan->layouts[cur], R, W) : 0;
+            const int count_cur = cur >= 0 ? walk(cur_S, nullptr, nullptr) : -1;
+            const uint32_t S_new = first_fit(cur_S);
+            const int count_new = walk(S_new, nullptr, nullptr);
+            int lay = cur;
+            uint32_t S = cur_S;
+            if (cur < 0 || count_new > count_cur) {
+                S = S_new;
+                lay = intern(lm.make(S, cur >= 0 ? &plan->layouts[cur] : nullptr));
+            }
+            taken.clear();
+            rest.clear();
+            walk(S, &taken, &rest);
             if (taken.empty()) return fail(HGM_ERR_INVALID, "phase scheduling made no progress");
             DevPhase ph;
-            ph.layout = best;
+            ph.layout = lay;
             ph.op_begin = (int)dev_ops.size();
-            emit_phase<Real>(ops, taken, best, R, W, loc_of, tmask, dev_ops);
+            emit_phase<Real>(ops, taken, Roles(plan->layouts[lay], R, W), R, loc_of, tmask, dev_ops);
             ph.op_end = (int)dev_ops.size();
-            int prev = cur < 0 ? (best == LAYOUT_A ? LAYOUT_A : LAYOUT_C) : cur;
-            ph.xwarp = (prev != best) && (prev == LAYOUT_A || best == LAYOUT_A) ? 1 : 0;
-            if (prev != best) plan->n_transposes++;
+            ph.xwarp = 0;
+            if (cur >= 0 && cur != lay) {
+                ph.xwarp = lm.same_warps(plan->layouts[cur], plan->layouts[lay]) ? 0 : 1;
+                plan->n_transposes++;
+            }
             plan->phases.push_back(ph);
-            cur = best;
+            cur = lay;
             pending.swap(rest);
         }
         pa.phase_end = (int)plan->phases.size();
-        const DevPhase &first = plan->phases[pa.phase_begin];
-        pa.load_layout = first.layout == LAYOUT_A ? LAYOUT_A : LAYOUT_C;
-        pa.store_layout = cur == LAYOUT_A ? LAYOUT_A : LAYOUT_C;
-        if (cur == LAYOUT_B || cur == LAYOUT_E) plan->n_transposes++;
+        // load and store layouts: the first and last phase's when coalesced,
+        // else one with the same warp bits and no low index bit in registers
+        DevPhase &first = plan->phases[pa.phase_begin];
+        pa.load_layout = first.layout;
+        if (!lm.coalesced(plan->layouts[first.layout])) {
+            const Lay f = plan->layouts[first.layout];
+            const uint32_t avoid = (1u << L) - 1;
+            uint32_t S0 = lm.fill(LayoutMaker::regs(f, R, W) & ~avoid, 0);
+            pa.load_layout = intern(lm.make(S0, &f));
+            first.xwarp = lm.same_warps(plan->layouts[pa.load_layout], f) ? 0 : 1;
+            plan->n_transposes++;
+        }
+        pa.store_layout = cur;
+        pa.store_xwarp = 0;
+        if (!lm.coalesced(plan->layouts[cur])) {
+            const Lay c = plan->layouts[cur];
+            const uint32_t avoid = (1u << L) - 1;
+            uint32_t S1 = lm.fill(LayoutMaker::regs(c, R, W) & ~avoid, 0);
+            pa.store_layout = intern(lm.make(S1, &c));
+            pa.store_xwarp = lm.same_warps(plan->layouts[pa.store_layout], c) ? 0 : 1;
+            plan->n_transposes++;
+        }
+        for (int k = 0; k < 5 + W + R; k++) {
+            pa.ld_gbit[k] = pa.tb[plan->layouts[pa.load_layout].pos[k]];
+            pa.st_gbit[k] = pa.tb[plan->layouts[pa.store_layout].pos[k]];
+        }
         plan->passes.push_back(pa);
         pass_index++;
     }

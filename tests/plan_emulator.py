@@ -16,9 +16,10 @@ import numpy as np
 from simulador_quantico_b200._lib import check, lib
 
 PASS_DT = np.dtype([("n", "<i4"), ("k", "<i4"), ("phase_begin", "<i4"), ("phase_end", "<i4"),
-                    ("load_layout", "<i4"), ("store_layout", "<i4"), ("flags", "<i4"), ("pad", "<i4"),
+                    ("load_layout", "<i4"), ("store_layout", "<i4"), ("flags", "<i4"), ("store_xwarp", "<i4"),
                     ("tb", "i1", 16), ("tile_mask", "<u8"), ("phases", "<u8"), ("ops", "<u8"),
-                    ("norm_out", "<u8"), ("scale_in", "<u8")])
+                    ("norm_out", "<u8"), ("scale_in", "<u8"), ("layouts", "<u8"), ("run_pos", "i1", 18),
+                    ("run_len", "i1", 18), ("nruns", "<i4"), ("ld_gbit", "i1", 16), ("st_gbit", "i1", 16)])
 PHASE_DT = np.dtype([("layout", "<i4"), ("op_begin", "<i4"), ("op_end", "<i4"), ("xwarp", "<i4")])
 
 
@@ -36,7 +37,6 @@ SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"
             "<f4": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f4", 8)])}
 
 K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK = range(9)
-LAYOUT_C, LAYOUT_B, LAYOUT_A, LAYOUT_E = 0, 1, 2, 3
 PB_F_ACTIVE = 1 << 16
 REG_BITS = {"f64": 4, "f32": 5}
 
@@ -52,32 +52,64 @@ def export(plan, precision):
     raw = C.string_at(ops, nb.value) if nb.value else b""
     odt = SMALL_DT[real] if sm.value else op_dtype(real)
     opsarr = np.frombuffer(raw, odt) if raw else np.zeros(0, odt)
-    return dict(passes=passes, phases=phases, ops=opsarr, W=wb.value, small=bool(sm.value))
+    lp, nl = C.c_void_p(), C.c_int64()
+    check(lib.hgm_plan_layouts(plan.h, C.byref(lp), C.byref(nl)))
+    layouts = (np.frombuffer(C.string_at(lp, nl.value * 16), np.int8).reshape(nl.value, 16).astype(np.int64)
+               if nl.value else np.zeros((0, 16), np.int64))
+    return dict(passes=passes, phases=phases, ops=opsarr, W=wb.value, small=bool(sm.value), layouts=layouts)
 
 
-def layout_coords(layout, R, W, K):
-    """For every local index j: (lane, warp, reg) in the given layout."""
+def layout_coords(pos, R, W, K):
+    """For every local index j: (lane, warp, reg) in the layout whose roles
+    (thread bits 0..4+W, then register bits) sit on local bits pos[...]."""
     j = np.arange(1 << K)
-    if layout == LAYOUT_C:
-        lane, reg, warp = j & 31, (j >> 5) & ((1 << R) - 1), j >> (5 + R)
-    elif layout == LAYOUT_B:
-        reg, lane, warp = j & ((1 << R) - 1), (j >> R) & 31, j >> (5 + R)
-    elif layout == LAYOUT_E:
-        lane = (j & 15) | (((j >> 8) & 1) << 4)
-        reg, warp = (j >> 4) & 15, j >> 9
-    else:
-        lane, warp, reg = j & 31, (j >> 5) & ((1 << W) - 1), (j >> (5 + W)) & ((1 << R) - 1)
-    return lane, warp, reg
+    thr = sum(((j >> int(pos[t])) & 1) << t for t in range(5 + W))
+    reg = sum(((j >> int(pos[5 + W + q])) & 1) << q for q in range(R))
+    return thr & 31, thr >> 5, reg
 
 
-def local_of(layout, R, W, lane, warp, reg):
-    if layout == LAYOUT_C:
-        return lane | (reg << 5) | (warp << (5 + R))
-    if layout == LAYOUT_B:
-        return reg | (lane << R) | (warp << (5 + R))
-    if layout == LAYOUT_E:
-        return (lane & 15) | (reg << 4) | ((lane >> 4) << 8) | (warp << 9)
-    return lane | (warp << 5) | (reg << (5 + W))
+def local_of(pos, R, W, lane, warp, reg):
+    thr = lane | (warp << 5)
+    j = sum(((thr >> t) & 1) << int(pos[t]) for t in range(5 + W))
+    return j | sum(((reg >> q) & 1) << int(pos[5 + W + q]) for q in range(R))
+
+
+def check_pass_layouts(e, pa, R, W, K):
+    """The kernel's assumptions about a pass's layouts: every layout is a
+    permutation of the K local bits; its low thread bits keep the padded
+    transposes free of bank conflicts; the load and store layouts move whole
+    runs of the low index bits; the global bits handed to the kernel match;
+    a transpose marked warp-local keeps every warp bit in place."""
+    nb = 3 if R == 4 else 4
+    per = {"<f8": 8, "<f4": 16}
+    lays = e["layouts"]
+    phases = e["phases"][pa["phase_begin"]:pa["phase_end"]]
+    used = {int(pa["load_layout"]), int(pa["store_layout"])} | {int(ph["layout"]) for ph in phases}
+    for li in used:
+        pos = lays[li][:5 + W + R]
+        assert sorted(pos.tolist()) == list(range(K)), pos
+        slots = {sum(((lane >> t) & 1) * ((1 << int(pos[t])) + ((1 << int(pos[t])) >> R)) for t in range(nb))
+                 % (1 << nb) for lane in range(1 << nb)}
+        assert len(slots) == 1 << nb, ("bank conflict", pos)
+    tb = [int(x) for x in pa["tb"][:K]]
+    for key, li in (("ld_gbit", int(pa["load_layout"])), ("st_gbit", int(pa["store_layout"]))):
+        pos = lays[li]
+        assert [int(x) for x in pa[key][:5 + W + R]] == [tb[int(pos[k])] for k in range(5 + W + R)]
+        low = 0
+        while low < K and tb[low] == low:
+            low += 1
+        for t in range(min(low, 3)):
+            assert int(pos[t]) == t, ("uncoalesced", key, pos)
+    cur = int(pa["load_layout"])
+
+    def same_warps(a, b):
+        return all(lays[a][5 + w] == lays[b][5 + w] for w in range(W))
+    for ph in phases:
+        if int(ph["layout"]) != cur and not int(ph["xwarp"]):
+            assert same_warps(cur, int(ph["layout"]))
+        cur = int(ph["layout"])
+    if cur != int(pa["store_layout"]) and not int(pa["store_xwarp"]):
+        assert same_warps(cur, int(pa["store_layout"]))
 
 
 def apply_small(state, ops, n):
@@ -179,6 +211,7 @@ def run(plan, precision, state, iterations=1):
     for _ in range(iterations):
         for pa in e["passes"]:
             K = int(pa["k"])
+            check_pass_layouts(e, pa, R, W, K)
             tb = [int(x) for x in pa["tb"][:K]]
             tmask = int(pa["tile_mask"])
             free = [g for g in range(n) if not (tmask >> g) & 1]
@@ -187,6 +220,13 @@ def run(plan, precision, state, iterations=1):
             base = np.zeros(T, dtype=np.int64)
             for k, g in enumerate(free):
                 base |= ((tiles >> k) & 1) << g
+            # the kernels deposit the tile number run by run
+            runs, shift = np.zeros(T, dtype=np.int64), 0
+            for i in range(int(pa["nruns"])):
+                ln, pos = int(pa["run_len"][i]), int(pa["run_pos"][i])
+                runs |= ((tiles >> shift) & ((1 << ln) - 1)) << pos
+                shift += ln
+            assert shift == len(free) and np.array_equal(runs, base)
             j = np.arange(1 << K, dtype=np.int64)
             scat = np.zeros(1 << K, dtype=np.int64)
             for q, g in enumerate(tb):
@@ -194,7 +234,7 @@ def run(plan, precision, state, iterations=1):
             gidx = base[:, None] | scat[None, :]
             tile = state[gidx]  # [T, 2^K] by local index
             for ph in e["phases"][pa["phase_begin"]:pa["phase_end"]]:
-                lay = int(ph["layout"])
+                lay = e["layouts"][int(ph["layout"])]
                 lane, warp, reg = layout_coords(lay, R, W, K)
                 thr = lane | (warp << 5)
                 recs = e["ops"][ph["op_begin"]:ph["op_end"]]
