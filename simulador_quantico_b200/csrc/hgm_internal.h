@@ -99,7 +99,8 @@ struct alignas(16) DevOp {
     int32_t kind, tpos;
     uint32_t cm_reg, cv_reg;   // controls on register bits
     uint32_t cm_thr, cv_thr;   // controls on thread bits (lane | warp << 5)
-    uint32_t pad0, pad1;
+    int32_t tpos2;             // tpos again, so a phase-block term's thread controls and
+    uint32_t pad1;             // target come in one 16-byte load
     uint64_t cm_glob, cv_glob; // controls on non-tile index bits
     Real m[8];
 };
@@ -193,6 +194,16 @@ struct State {
 
 // ---- launchers (kernels.cu) ----------------------------------------------------
 int launch_plan(State *s, const Plan *p, int iterations, void *stream);
+// The same in pieces: queues up to max_launches more launches of the plan
+// from cursor c (which carries the renormalisation slots across calls).
+struct PlanCursor {
+    int64_t next = 0;
+    int slot = 0;
+    bool scale_next = false;
+    int scale_slot = 0;
+};
+int launch_plan_steps(State *s, const Plan *p, int iterations, PlanCursor *c, int64_t max_launches, void *stream);
+int64_t plan_launches(const Plan *p, int iterations);
 int launch_set_basis(State *s, int64_t index, void *stream);
 int reduce_norm(State *s, double *out, void *stream);
 int reduce_prob_one(State *s, int bit, double *out, void *stream);

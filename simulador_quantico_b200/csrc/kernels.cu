@@ -173,7 +173,7 @@ static int launch_small(State *s, const Plan *p, int iterations, cudaStream_t st
     return check("small_kernel launch");
 }
 
-int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
+int launch_plan_steps(State *s, const Plan *p, int iterations, PlanCursor *c, int64_t max_launches, void *stream) {
     if (s->qubits != p->qubits) return fail(HGM_ERR_INVALID, "plan is for %d qubits, state has %d", p->qubits, s->qubits);
     if (s->precision != p->precision) return fail(HGM_ERR_INVALID, "plan and state precision differ");
     // every device pointer a launch passes must exist: an op list that was
@@ -184,39 +184,47 @@ int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
         return fail(HGM_ERR_INVALID, "plan used before upload_plan");
     cudaStream_t st = pick(stream);
     if (!st) return HGM_ERR_CUDA;
-    if (p->small) return p->n_small_ops ? (p->precision == HGM_F64 ? launch_small<double>(s, p, iterations, st)
-                                                                 : launch_small<float>(s, p, iterations, st))
-                                       : HGM_OK;
-    const size_t np = p->passes.size();
+    if (p->small) {
+        if (c->next > 0 || max_launches < 1) return HGM_OK;
+        c->next = 1;
+        return p->n_small_ops ? (p->precision == HGM_F64 ? launch_small<double>(s, p, iterations, st)
+                                                         : launch_small<float>(s, p, iterations, st))
+                              : HGM_OK;
+    }
+    const int64_t np = (int64_t)p->passes.size();
     const int R = p->renorm_every;
-    int64_t global_pass = 0;
-    const int64_t total = (int64_t)np * iterations;
-    int slot = 0;
-    bool scale_next = false;
-    int scale_slot = 0;
-    for (int it = 0; it < iterations; it++) {
-        for (size_t i = 0; i < np; i++, global_pass++) {
-            PassArgs pa = p->passes[i];
-            pa.flags = 0;
-            if (scale_next) {
-                pa.flags |= PASS_SCALE;
-                pa.scale_in = p->d_norm + scale_slot;
-                scale_next = false;
-            }
-            if (R > 0 && ((global_pass + 1) % R == 0) && global_pass + 1 < total) {
-                pa.flags |= PASS_NORM;
-                pa.norm_out = p->d_norm + slot;
-                cudaMemsetAsync(pa.norm_out, 0, sizeof(double), st);
-                scale_next = true;
-                scale_slot = slot;
-                slot = (slot + 1) % 64;
-            }
-            int rc = p->precision == HGM_F64 ? launch_pass_w<double>(p->warp_bits, s->d, pa, st)
-                                             : launch_pass_w<float>(p->warp_bits, s->d, pa, st);
-            if (rc) return rc;
+    const int64_t total = np * iterations;
+    for (int64_t k = 0; k < max_launches && c->next < total; k++, c->next++) {
+        const int64_t g = c->next;
+        PassArgs pa = p->passes[g % np];
+        pa.flags = 0;
+        if (c->scale_next) {
+            pa.flags |= PASS_SCALE;
+            pa.scale_in = p->d_norm + c->scale_slot;
+            c->scale_next = false;
         }
+        if (R > 0 && ((g + 1) % R == 0) && g + 1 < total) {
+            pa.flags |= PASS_NORM;
+            pa.norm_out = p->d_norm + c->slot;
+            cudaMemsetAsync(pa.norm_out, 0, sizeof(double), st);
+            c->scale_next = true;
+            c->scale_slot = c->slot;
+            c->slot = (c->slot + 1) % 64;
+        }
+        int rc = p->precision == HGM_F64 ? launch_pass_w<double>(p->warp_bits, s->d, pa, st)
+                                         : launch_pass_w<float>(p->warp_bits, s->d, pa, st);
+        if (rc) return rc;
     }
     return check("pass_kernel launch");
+}
+
+int64_t plan_launches(const Plan *p, int iterations) {
+    return p->small ? 1 : (int64_t)p->passes.size() * iterations;
+}
+
+int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
+    PlanCursor c;
+    return launch_plan_steps(s, p, iterations, &c, plan_launches(p, iterations), stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -455,31 +455,24 @@ __device__ __forceinline__ float2 load_c<float, float2>(const float *__restrict_
     return __ldg(reinterpret_cast<const float2 *>(p));
 }
 
-// Hides a pointer's value from the scheduler so the next term's descriptor
-// loads are issued only after this point: without it, ptxas hoists the loads
-// of every unrolled term and runs out of registers.
-template <typename T>
-__device__ __forceinline__ const T *opaque(const T *p) {
-    asm volatile("" : "+l"(p));
-    return p;
-}
-
+// Factor of one phase-block term for this thread: d0 or d1 of its diagonal
+// gate by the value of its target (a thread or non-tile bit), or 1 when its
+// controls on thread and non-tile bits do not hold.  Branch-free: the
+// conditions differ between threads of a warp.
 template <typename Real, typename A2>
-__device__ __forceinline__ bool term_factor(const DevOp<Real> *__restrict__ t, uint64_t base, uint32_t thr, A2 &f0,
-                                            A2 &f1) {
-    t = opaque(t);
-    const uint2 th = __ldg(reinterpret_cast<const uint2 *>(&t->cm_thr));
-    const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(&t->cm_glob));
-    if ((base & gl.x) != gl.y || (thr & th.x) != th.y) return false;
-    const int tpos = __ldg(&t->tpos);
-    f0 = load_c<Real, A2>(t->m);
-    f1 = load_c<Real, A2>(t->m + 6);
-    if (tpos >= TPOS_THREAD) {  // target outside the registers: pick this thread's entry
-        const int bv = tpos >= TPOS_GLOBAL ? (int)((base >> (tpos - TPOS_GLOBAL)) & 1)
-                                           : (int)((thr >> (tpos - TPOS_THREAD)) & 1);
-        if (bv) f0 = f1;
-    }
-    return true;
+__device__ __forceinline__ A2 term_factor(const DevOp<Real> *__restrict__ t, uint64_t base, uint32_t thr) {
+    const uint4 th = __ldg(reinterpret_cast<const uint4 *>(t) + 1);  // cm_thr, cv_thr, tpos2
+    const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(t) + 2);
+    const A2 f0 = load_c<Real, A2>(t->m), f1 = load_c<Real, A2>(t->m + 6);
+    const bool ok = ((base & gl.x) == gl.y) && ((thr & th.x) == th.y);
+    const int tp = (int)th.z;
+    const uint32_t bv = tp >= TPOS_GLOBAL   ? (uint32_t)(base >> (tp - TPOS_GLOBAL)) & 1u
+                        : tp >= TPOS_THREAD ? (thr >> (tp - TPOS_THREAD)) & 1u
+                                            : 0u;
+    A2 f = bv ? f1 : f0;
+    f.x = ok ? f.x : (Real)1;
+    f.y = ok ? f.y : (Real)0;
+    return f;
 }
 
 template <typename Real, typename A2>
@@ -488,6 +481,45 @@ __device__ __forceinline__ A2 cmul2(A2 a, A2 b) {
     o.x = a.x * b.x - a.y * b.y;
     o.y = a.x * b.y + a.y * b.x;
     return o;
+}
+
+// acc times the factors of terms t[0..n), two terms per step (two chains, so
+// that one term's loads overlap the other's arithmetic).
+template <typename Real, typename A2>
+__device__ __forceinline__ A2 term_product(const DevOp<Real> *__restrict__ t, int n, uint64_t base, uint32_t thr,
+                                           A2 acc) {
+    A2 acc2;
+    acc2.x = 1;
+    acc2.y = 0;
+    int i = 0;
+#pragma unroll 1
+    for (; i + 1 < n; i += 2) {
+        const A2 fa = term_factor<Real, A2>(t + i, base, thr), fb = term_factor<Real, A2>(t + i + 1, base, thr);
+        acc = cmul2<Real>(acc, fa);
+        acc2 = cmul2<Real>(acc2, fb);
+    }
+    if (i < n) acc = cmul2<Real>(acc, term_factor<Real, A2>(t + i, base, thr));
+    return cmul2<Real>(acc, acc2);
+}
+
+// D terms (a diagonal gate on register bit b, controls elsewhere): h takes
+// d0, g takes d1, where the controls hold.
+template <typename Real, typename A2>
+__device__ __forceinline__ void term_diag_product(const DevOp<Real> *__restrict__ t, int n, uint64_t base,
+                                                  uint32_t thr, A2 &h, A2 &g) {
+#pragma unroll 1
+    for (int i = 0; i < n; i++) {
+        const uint4 th = __ldg(reinterpret_cast<const uint4 *>(t + i) + 1);
+        const ulonglong2 gl = __ldg(reinterpret_cast<const ulonglong2 *>(t + i) + 2);
+        A2 f0 = load_c<Real, A2>(t[i].m), f1 = load_c<Real, A2>(t[i].m + 6);
+        const bool ok = ((base & gl.x) == gl.y) && ((thr & th.x) == th.y);
+        f0.x = ok ? f0.x : (Real)1;
+        f0.y = ok ? f0.y : (Real)0;
+        f1.x = ok ? f1.x : (Real)1;
+        f1.y = ok ? f1.y : (Real)0;
+        h = cmul2<Real>(h, f0);
+        g = cmul2<Real>(g, f1);
+    }
 }
 
 // Byte K of the 16 phase-block term counts, kept packed in four words.
@@ -509,27 +541,11 @@ struct PhaseBits {
                                                uint32_t thr, uint32_t xr) {
         const int ng = count_byte<1 + B>(cnt), nh = count_byte<1 + R + B>(cnt), nd = count_byte<1 + 2 * R + B>(cnt);
         if (act & (1u << B)) {
-            A2 g = carry, h = carry;
+            A2 g = term_product<Real, A2>(t, ng, base, thr, carry);
+            A2 h = term_product<Real, A2>(t + ng, nh, base, thr, carry);
             carry.x = 1;
             carry.y = 0;
-#pragma unroll 1
-            for (int i = 0; i < ng; i++) {
-                A2 f0, f1;
-                if (term_factor<Real>(t + i, base, thr, f0, f1)) g = cmul2<Real>(g, f0);
-            }
-#pragma unroll 1
-            for (int i = 0; i < nh; i++) {
-                A2 f0, f1;
-                if (term_factor<Real>(t + ng + i, base, thr, f0, f1)) h = cmul2<Real>(h, f0);
-            }
-#pragma unroll 1
-            for (int i = 0; i < nd; i++) {
-                A2 f0, f1;
-                if (term_factor<Real>(t + ng + nh + i, base, thr, f0, f1)) {
-                    h = cmul2<Real>(h, f0);
-                    g = cmul2<Real>(g, f1);
-                }
-            }
+            term_diag_product<Real, A2>(t + ng + nh, nd, base, thr, h, g);
             // g belongs to the registers whose label has bit B set
             const bool flip = (xr >> B) & 1u;
             const A2 g1 = flip ? h : g, h1 = flip ? g : h;
@@ -562,11 +578,7 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
     carry.x = 1;
     carry.y = 0;
     const int nf = count_byte<0>(cnt);
-#pragma unroll 1
-    for (int i = 0; i < nf; i++) {
-        A2 f0, f1;
-        if (term_factor<Real>(t + i, base, thr, f0, f1)) carry = cmul2<Real>(carry, f0);
-    }
+    carry = term_product<Real, A2>(t, nf, base, thr, carry);
     PhaseBits<Real, A2, R, 0>::run(a, t + nf, cnt, act, carry, base, thr, xr);
     if ((act & PB_F_ACTIVE) && !(act & ((1u << R) - 1u))) {
 #pragma unroll

@@ -227,6 +227,7 @@ DevOp<Real> encode(const SOp &o, const Roles &ro, const int loc_of[64], uint64_t
         const Role rl = ro.of[loc_of[g]];
         d.tpos = rl.kind == ROLE_REG ? rl.idx : TPOS_THREAD + rl.idx;
     }
+    d.tpos2 = d.tpos;
     for (int k = 0; k < 4; k++) {
         d.m[2 * k] = (Real)m[k].real();
         d.m[2 * k + 1] = (Real)m[k].imag();

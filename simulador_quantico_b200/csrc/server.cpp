@@ -61,9 +61,20 @@ struct Request {
     int64_t argmax = -1;
 };
 
+// Passes are queued on a slot's stream in chunks, at most two chunks ahead
+// of the GPU: a long plan (a Grover circuit is thousands of passes) then
+// neither fills the launch queue -- where the worker would block, and every
+// other slot with it -- nor starves the slots admitted after it.
+constexpr int64_t kChunkLaunches = 32;
+
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    cudaEvent_t chunk[2] = {nullptr, nullptr};
+    int chunks_in_flight = 0, chunk_next = 0;
+    PlanCursor cursor;
+    int64_t total = 0;   // launches of the request's plan
+    bool tail = false;   // reductions and result copy queued (s.done recorded)
     double *partials = nullptr;
     long long *ibest = nullptr;
     double *dres = nullptr;   // 4 doubles
@@ -118,6 +129,8 @@ struct Server {
             if (s.dres) cudaFree(s.dres);
             if (s.hres) cudaFreeHost(s.hres);
             if (s.done) cudaEventDestroy(s.done);
+            for (cudaEvent_t ev : s.chunk)
+                if (ev) cudaEventDestroy(ev);
             if (s.stream) cudaStreamDestroy(s.stream);
         }
         for (Request *r : queue) delete r;
@@ -171,14 +184,39 @@ struct Server {
         if (e != cudaSuccess) return fail(HGM_ERR_NOMEM, "request state: %s", cudaGetErrorString(e));
         r->state.qubits = r->n;
         r->state.precision = opts.precision;
+        s.cursor = PlanCursor();
+        s.total = plan_launches(r->plan, 1);
+        s.chunks_in_flight = 0;
+        s.tail = false;
         int rc = launch_set_basis(&r->state, r->init_index, s.stream);
-        if (!rc) rc = launch_plan(&r->state, r->plan, 1, s.stream);
-        if (!rc) rc = launch_norm_async(&r->state, s.partials, s.dres, s.stream);
-        if (!rc && r->result_mask) rc = launch_argmax_async(&r->state, r->result_mask, s.partials, s.ibest, s.dres + 2, s.stream);
-        if (rc) return rc;
-        cudaMemcpyAsync(s.hres, s.dres, 4 * sizeof(double), cudaMemcpyDeviceToHost, s.stream);
-        e = cudaEventRecord(s.done, s.stream);
-        return e == cudaSuccess ? HGM_OK : fail(HGM_ERR_CUDA, "event record: %s", cudaGetErrorString(e));
+        return rc ? rc : feed(s);
+    }
+
+    // Queues the slot's next chunks (while fewer than two are in flight) and,
+    // after the last pass, the reductions, the result copy and s.done.
+    int feed(Slot &s) {
+        Request *r = s.req;
+        while (!s.tail && s.chunks_in_flight < 2) {
+            if (s.cursor.next < s.total) {
+                int rc = launch_plan_steps(&r->state, r->plan, 1, &s.cursor, kChunkLaunches, s.stream);
+                if (rc) return rc;
+                cudaError_t e = cudaEventRecord(s.chunk[s.chunk_next], s.stream);
+                if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "event record: %s", cudaGetErrorString(e));
+                s.chunk_next ^= 1;
+                s.chunks_in_flight++;
+            }
+            if (s.cursor.next >= s.total) {
+                int rc = launch_norm_async(&r->state, s.partials, s.dres, s.stream);
+                if (!rc && r->result_mask)
+                    rc = launch_argmax_async(&r->state, r->result_mask, s.partials, s.ibest, s.dres + 2, s.stream);
+                if (rc) return rc;
+                cudaMemcpyAsync(s.hres, s.dres, 4 * sizeof(double), cudaMemcpyDeviceToHost, s.stream);
+                cudaError_t e = cudaEventRecord(s.done, s.stream);
+                if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "event record: %s", cudaGetErrorString(e));
+                s.tail = true;
+            }
+        }
+        return HGM_OK;
     }
 
     int device = 0;
@@ -239,7 +277,27 @@ struct Server {
             // completions
             for (Slot &s : slots) {
                 if (!s.req) continue;
-                cudaError_t q = cudaEventQuery(s.done);
+                cudaError_t q;
+                if (!s.tail) {
+                    // retire the oldest chunk if it has run, then queue more
+                    const int oldest = (s.chunk_next + 2 - s.chunks_in_flight) & 1;
+                    q = s.chunks_in_flight ? cudaEventQuery(s.chunk[oldest]) : cudaSuccess;
+                    if (q == cudaSuccess) {
+                        if (s.chunks_in_flight) s.chunks_in_flight--;
+                        int rc = feed(s);
+                        if (rc) {
+                            s.req->status = rc;
+                            cudaStreamSynchronize(s.stream);
+                            finish(s);
+                        }
+                        progress = true;
+                        continue;
+                    }
+                    if (q == cudaErrorNotReady) continue;
+                    // a chunk failed: reported below like a failed request
+                } else {
+                    q = cudaEventQuery(s.done);  // s.done belongs to this request once the tail is queued
+                }
                 if (q == cudaSuccess) {
                     finish(s);
                     progress = true;
@@ -317,6 +375,8 @@ int hgm_server_create(const hgm_server_opts *opts, hgm_server **out) {
         cudaError_t e;
         if ((e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&sl.chunk[0], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&sl.chunk[1], cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaMalloc(&sl.partials, 2 * REDUCE_SCRATCH_BLOCKS * sizeof(double))) != cudaSuccess ||
             (e = cudaMalloc(&sl.ibest, REDUCE_SCRATCH_BLOCKS * sizeof(long long))) != cudaSuccess ||
             (e = cudaMalloc(&sl.dres, 4 * sizeof(double))) != cudaSuccess ||

@@ -25,7 +25,7 @@ PHASE_DT = np.dtype([("layout", "<i4"), ("op_begin", "<i4"), ("op_end", "<i4"), 
 
 def op_dtype(real):
     fields = [("kind", "<i4"), ("tpos", "<i4"), ("cm_reg", "<u4"), ("cv_reg", "<u4"), ("cm_thr", "<u4"),
-              ("cv_thr", "<u4"), ("pad0", "<u4"), ("pad1", "<u4"), ("cm_glob", "<u8"), ("cv_glob", "<u8"),
+              ("cv_thr", "<u4"), ("tpos2", "<i4"), ("pad1", "<u4"), ("cm_glob", "<u8"), ("cv_glob", "<u8"),
               ("m", real, 8)]
     dt = np.dtype(fields)
     size = (dt.itemsize + 15) // 16 * 16
