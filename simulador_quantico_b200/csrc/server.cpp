@@ -8,13 +8,20 @@
 //     slot is free and the request's state bytes (16*2^n FP64, 8*2^n FP32)
 //     fit the HBM budget (a request larger than the whole budget is refused);
 //   * gives each admitted request a slot -- a CUDA stream with its own
-//     reduction scratch -- allocates the state stream-ordered
-//     (cudaMallocAsync from the device's memory pool, so no allocation
-//     synchronises the device), initialises it, queues the plan's passes, an
-//     FP64 norm and (if asked) the marginal argmax, copies those few numbers
-//     to pinned host memory and records an event;
+//     reduction scratch -- and a state buffer from the server's cache of
+//     device buffers, initialises it, queues the plan's passes, an FP64 norm
+//     and (if asked) the marginal argmax, copies those few numbers to pinned
+//     host memory and records an event;
 //   * polls the slots' events; a finished request records its completion
-//     time, frees (or keeps) its state and frees the slot for the next one.
+//     time, returns (or keeps) its state buffer and frees the slot for the
+//     next one.
+// State sizes are powers of two, so finished states are kept by size and
+// handed to the next request of that size: after warm-up the worker makes
+// no allocation calls.  (Allocating from the stream-ordered pool per request
+// blocked the worker, and with it every slot, for up to half a second when
+// the pool had to map memory for a 1-2 GiB state.)  New buffers are
+// cudaMalloc'ed while admitted plus cached bytes stay within the budget;
+// cached buffers of other sizes are freed first when they would not.
 // Requests on different slots run concurrently on the device; new requests
 // are admitted while earlier ones are still executing.  A request's result
 // does not depend on what else runs: it uses its own plan, state and scratch
@@ -84,8 +91,59 @@ struct Slot {
 
 }  // namespace
 
+// Device buffers for request states, cached by size.  Worker and client
+// threads both return buffers, so it has its own lock.
+struct StateCache {
+    std::mutex mu;
+    std::map<int64_t, std::vector<void *>> free_by_size;
+    int64_t cached = 0;  // bytes held in free_by_size
+
+    // A buffer of `bytes`; `others` = bytes the server holds outside the
+    // cache (admitted states, this one included), `budget` their limit.
+    int acquire(int64_t bytes, int64_t others, int64_t budget, void **out) {
+        std::lock_guard<std::mutex> lk(mu);
+        auto &v = free_by_size[bytes];
+        if (!v.empty()) {
+            *out = v.back();
+            v.pop_back();
+            cached -= bytes;
+            return HGM_OK;
+        }
+        // make room: free cached buffers, largest first, while over budget
+        while (others + cached > budget && cached > 0) evict_largest();
+        cudaError_t e = cudaMalloc(out, (size_t)bytes);
+        if (e != cudaSuccess && cached > 0) {
+            cudaGetLastError();
+            while (cached > 0) evict_largest();
+            e = cudaMalloc(out, (size_t)bytes);
+        }
+        return e == cudaSuccess ? HGM_OK : fail(HGM_ERR_NOMEM, "request state: %s", cudaGetErrorString(e));
+    }
+    // The GPU must be done with the buffer.
+    void release(void *p, int64_t bytes) {
+        std::lock_guard<std::mutex> lk(mu);
+        free_by_size[bytes].push_back(p);
+        cached += bytes;
+    }
+    void evict_largest() {
+        for (auto it = free_by_size.rbegin(); it != free_by_size.rend(); ++it)
+            if (!it->second.empty()) {
+                cudaFree(it->second.back());
+                it->second.pop_back();
+                cached -= it->first;
+                return;
+            }
+        cached = 0;
+    }
+    ~StateCache() {
+        for (auto &kv : free_by_size)
+            for (void *p : kv.second) cudaFree(p);
+    }
+};
+
 struct Server {
     hgm_server_opts opts;
+    StateCache cache;
     std::mutex mu;
     std::condition_variable cv;
     std::deque<Request *> queue;
@@ -121,7 +179,7 @@ struct Server {
         for (Slot &s : slots) {
             if (s.stream) cudaStreamSynchronize(s.stream);
             if (s.req) {
-                if (s.req->state.d) cudaFreeAsync(s.req->state.d, s.stream);
+                if (s.req->state.d) cudaFree(s.req->state.d);
                 delete s.req;
             }
             if (s.partials) cudaFree(s.partials);
@@ -135,7 +193,7 @@ struct Server {
         }
         for (Request *r : queue) delete r;
         for (auto &kv : kept) {
-            if (kv.second->state.d) cudaFreeAsync(kv.second->state.d, (cudaStream_t)default_stream());
+            if (kv.second->state.d) cudaFree(kv.second->state.d);
             delete kv.second;
         }
     }
@@ -162,7 +220,7 @@ struct Server {
             std::lock_guard<std::mutex> lk(mu);
             kept[r->id] = r;
         } else {
-            cudaFreeAsync(r->state.d, s.stream);
+            if (r->state.d) cache.release(r->state.d, r->bytes);  // s.done has completed: the GPU is done with it
             r->state.d = nullptr;
             std::lock_guard<std::mutex> lk(mu);
             bytes_in_use -= r->bytes;
@@ -180,8 +238,13 @@ struct Server {
     int start(Slot &s, Request *r) {
         r->t_admit = now_s();
         s.req = r;
-        cudaError_t e = cudaMallocAsync(&r->state.d, (size_t)r->bytes, s.stream);
-        if (e != cudaSuccess) return fail(HGM_ERR_NOMEM, "request state: %s", cudaGetErrorString(e));
+        int64_t held;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            held = bytes_in_use;
+        }
+        int arc = cache.acquire(r->bytes, held, opts.budget_bytes, &r->state.d);
+        if (arc) return arc;
         r->state.qubits = r->n;
         r->state.precision = opts.precision;
         s.cursor = PlanCursor();
@@ -362,14 +425,6 @@ int hgm_server_create(const hgm_server_opts *opts, hgm_server **out) {
     if (!default_stream()) return HGM_ERR_CUDA;
     std::unique_ptr<Server> s(new Server());
     s->opts = *opts;
-    // keep freed request memory in the pool up to the budget (no trimming on every free)
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t thr = (uint64_t)opts->budget_bytes;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
     s->slots.resize(opts->max_inflight);
     for (Slot &sl : s->slots) {
         cudaError_t e;
@@ -498,7 +553,9 @@ int hgm_server_release(hgm_server *ss, int64_t id) {
         s->kept.erase(it);
         s->bytes_in_use -= r->bytes;
     }
-    cudaFreeAsync(r->state.d, (cudaStream_t)default_stream());
+    // the caller may still have work on the library stream that reads it
+    cudaStreamSynchronize((cudaStream_t)default_stream());
+    if (r->state.d) s->cache.release(r->state.d, r->bytes);
     delete r;
     s->cv.notify_all();
     return HGM_OK;
