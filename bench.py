@@ -52,10 +52,11 @@ FALLBACK_HBM_GBS = 6650.0
 
 # DRAM bytes read + written per pass-kernel launch, over the algorithmic 2*S,
 # from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of two
-# passes of the 26-qubit random layered circuit: FP32 1.019 GB and FP64
-# 2.096 GB per launch against 1.074 / 2.147 GB.  Writes come out a little
-# short because the last lines are still in L2 when the launch ends.
-TRAFFIC_OVER_ALGO = {"f32": 0.949, "f64": 0.976}
+# passes of the 26-qubit random layered circuit (FP32 1.017 GB and FP64
+# 2.093 GB per launch against 1.074 / 2.147 GB) and of two passes of the
+# 28-qubit Hadamard layer (8.555 GB against 8.590 GB).  Writes come out a
+# little short because the last lines are still in L2 when the launch ends.
+TRAFFIC_OVER_ALGO = {"f32": 0.947, "f64": 0.975, "f64_hadamard": 0.996}
 
 
 def hbm_peak():
@@ -326,8 +327,9 @@ def workload_hadamard(args, dist, sq):
                      "ok": bool(abs(p0 - (0.5 if runs % 2 else 0.0)) < 1e-9)}
     line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(achieved / peak, 4),
-                        "traffic": round(TRAFFIC_OVER_ALGO["f64"] * 2 * S / 1e9, 3), "traffic_unit": "GB per launch",
-                        "traffic_source": "ncu capture of the 26-qubit FP64 layered case, scaled to this state size",
+                        "traffic": round(TRAFFIC_OVER_ALGO["f64_hadamard"] * 2 * S / 1e9, 3),
+                        "traffic_unit": "GB per launch",
+                        "traffic_source": "ncu capture of the 28-qubit Hadamard layer, scaled to this state size",
                         "peak_source": peak_kind,
                         "kernel": "pass_kernel<double,%d,%d>" % (stats["reg_bits"], stats["warp_bits"]),
                         "algorithmic_bytes_per_launch": 2 * S}

@@ -99,6 +99,8 @@ int hgm_plan_create(const hgm_circuit *c, int qubits, const hgm_plan_opts *opts,
 /* Same, from a reference-layout NULL-terminated PT list (hgm_ref_pt**). */
 int hgm_plan_create_from_ref_pts(void *const *pts, int pt_precision, int qubits, const hgm_plan_opts *opts,
                                  hgm_plan **out);
+/* Waits for the work queued on the device, then frees the plan: a plan may be
+ * freed right after the executions that use it are queued. */
 void hgm_plan_free(hgm_plan *p);
 /* Plan statistics: ops after fusion, passes, phases, transposes. */
 int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes);
@@ -116,6 +118,7 @@ int hgm_plan_layouts(const hgm_plan *p, const int8_t **pos, int64_t *n_layouts);
 /* ---- device-resident states -------------------------------------------- */
 
 int hgm_state_create(int qubits, int precision, hgm_state **out);
+/* Waits for the work queued on the device, then frees the state. */
 void hgm_state_free(hgm_state *s);
 int hgm_state_qubits(const hgm_state *s);
 int hgm_state_precision(const hgm_state *s);

@@ -189,6 +189,7 @@ struct Batch {
     // Drops everything finalize built (plans, arena, tables, graph); the
     // circuits stay, so the batch can be finalized again with other settings.
     void release() {
+        if (graph || arena) cudaDeviceSynchronize();  // a replay may still be running
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
         for (void *p : {(void *)arena, (void *)d_tasks, (void *)d_next, (void *)d_done, (void *)d_error,

@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 
 #include "hgm_b200.h"
@@ -28,7 +29,30 @@ static const int kPrecision = HGM_F32;
 namespace {
 
 std::mutex g_mu;
-hgm_state *g_state = nullptr;
+
+// Device states kept between calls, by qubit count.  Callers that run many
+// circuits of a few sizes (the batched comparison) would otherwise pay a
+// device allocation and free per call, more than a small circuit's run.
+// At most kKeepBytes are kept; a state that does not fit replaces the rest.
+constexpr int64_t kKeepBytes = int64_t(4) << 30;
+std::map<int, hgm_state *> g_states;
+int64_t g_kept = 0;
+
+hgm_state *state_for(int qubits) {
+    auto it = g_states.find(qubits);
+    if (it != g_states.end()) return it->second;
+    const int64_t bytes = (int64_t(1) << qubits) * (int64_t)sizeof(hgm_dropin_amp);
+    if (g_kept + bytes > kKeepBytes) {
+        for (auto &kv : g_states) hgm_state_free(kv.second);
+        g_states.clear();
+        g_kept = 0;
+    }
+    hgm_state *st = nullptr;
+    if (hgm_state_create(qubits, kPrecision, &st)) return nullptr;
+    g_states[qubits] = st;
+    g_kept += bytes;
+    return st;
+}
 
 [[noreturn]] void die(const char *what) {
     printf("hgm_b200: %s: %s\n", what, hgm_last_error());
@@ -77,15 +101,12 @@ hgm_dropin_amp *GpuExecutionWrapper(hgm_dropin_amp *read_memory, hgm_ref_pt **pt
     hgm_plan *plan = nullptr;
     if (hgm_plan_create_from_ref_pts(reinterpret_cast<void *const *>(pts), kPrecision, qubits, &opts, &plan))
         die("planning");
-    if (g_state && (hgm_state_qubits(g_state) != qubits)) {
-        hgm_state_free(g_state);
-        g_state = nullptr;
-    }
-    if (!g_state && hgm_state_create(qubits, kPrecision, &g_state)) die("state allocation");
+    hgm_state *state = state_for(qubits);
+    if (!state) die("state allocation");
     const int64_t bytes = (int64_t(1) << qubits) * (int64_t)sizeof(hgm_dropin_amp);
-    if (hgm_state_upload(g_state, read_memory, bytes)) die("copy to device");
-    if (hgm_execute(g_state, plan, iterations, nullptr)) die("execution");
-    if (hgm_state_download(g_state, read_memory, bytes)) die("copy to host");
+    if (hgm_state_upload(state, read_memory, bytes)) die("copy to device");
+    if (hgm_execute(state, plan, iterations, nullptr)) die("execution");
+    if (hgm_state_download(state, read_memory, bytes)) die("copy to host");
     hgm_plan_free(plan);
 
     if (debug) {

@@ -103,7 +103,12 @@ int hgm_plan_create_from_ref_pts(void *const *pts, int pt_precision, int qubits,
     return finish_plan(ops, qubits, opts, out);
 }
 
-void hgm_plan_free(hgm_plan *p) { delete reinterpret_cast<Plan *>(p); }
+void hgm_plan_free(hgm_plan *p) {
+    Plan *pl = reinterpret_cast<Plan *>(p);
+    // launches are asynchronous: the plan's device records may still be in use
+    if (pl && (pl->d_ops || pl->d_phases)) cudaDeviceSynchronize();
+    delete pl;
+}
 
 int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes) {
     if (!p) return fail(HGM_ERR_INVALID, "null plan");
@@ -158,7 +163,10 @@ int hgm_state_create(int qubits, int precision, hgm_state **out) {
 void hgm_state_free(hgm_state *s) {
     State *st = reinterpret_cast<State *>(s);
     if (!st || !st->owned) return;  // views are released by their owner
-    if (st->d) cudaFree(st->d);
+    if (st->d) {
+        cudaDeviceSynchronize();  // work queued on the state may still be running
+        cudaFree(st->d);
+    }
     delete st;
 }
 

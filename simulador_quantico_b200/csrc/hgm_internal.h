@@ -2,6 +2,8 @@
 // translation units.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <complex>
 #include <cstdint>
 #include <map>
@@ -152,6 +154,15 @@ struct SmallOp {
 };
 
 // ---- plan ------------------------------------------------------------------
+// Where a plan's device records come from: cudaMalloc/cudaFree by default, or
+// an owner's cache (the server recycles them, so that serving makes no
+// allocation calls once warm).
+struct DevAllocator {
+    virtual cudaError_t alloc(void **p, size_t bytes) = 0;
+    virtual void free(void *p, size_t bytes) = 0;
+    virtual ~DevAllocator() {}
+};
+
 struct Plan {
     int precision = HGM_F64;
     int qubits = 0;
@@ -164,7 +175,9 @@ struct Plan {
     std::vector<unsigned char> ops_bytes;   // DevOp<Real>[] or SmallOp<Real>[]
     int64_t n_small_ops = 0;
     int64_t n_ops = 0, n_transposes = 0;
-    // device copies
+    // device copies, and their sizes as allocated
+    DevAllocator *allocator = nullptr;
+    size_t d_bytes[4] = {0, 0, 0, 0};  // ops, phases, layouts, norm
     void *d_phases = nullptr;
     void *d_layouts = nullptr;
     void *d_ops = nullptr;

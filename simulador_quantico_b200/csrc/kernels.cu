@@ -231,11 +231,18 @@ int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
 // plan upload
 // ---------------------------------------------------------------------------
 
+static cudaError_t plan_alloc(Plan *p, int k, void **out, size_t bytes) {
+    p->d_bytes[k] = bytes;
+    return p->allocator ? p->allocator->alloc(out, bytes) : cudaMalloc(out, bytes);
+}
+
 Plan::~Plan() {
-    if (d_phases) cudaFree(d_phases);
-    if (d_layouts) cudaFree(d_layouts);
-    if (d_ops) cudaFree(d_ops);
-    if (d_norm) cudaFree(d_norm);
+    void *ptrs[4] = {d_ops, d_phases, d_layouts, d_norm};
+    for (int k = 0; k < 4; k++) {
+        if (!ptrs[k]) continue;
+        if (allocator) allocator->free(ptrs[k], d_bytes[k]);
+        else cudaFree(ptrs[k]);
+    }
 }
 
 int upload_plan(Plan *p) {
@@ -243,14 +250,14 @@ int upload_plan(Plan *p) {
     if (ensure_ctx()) return HGM_ERR_CUDA;
     cudaError_t e;
     if (!p->ops_bytes.empty()) {
-        if ((e = cudaMalloc(&p->d_ops, p->ops_bytes.size())) != cudaSuccess)
+        if ((e = plan_alloc(p, 0, &p->d_ops, p->ops_bytes.size())) != cudaSuccess)
             return fail(HGM_ERR_NOMEM, "plan ops: %s", cudaGetErrorString(e));
         if ((e = cudaMemcpy(p->d_ops, p->ops_bytes.data(), p->ops_bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return fail(HGM_ERR_CUDA, "plan ops copy: %s", cudaGetErrorString(e));
     }
     if (!p->phases.empty()) {
         size_t b = p->phases.size() * sizeof(DevPhase);
-        if ((e = cudaMalloc(&p->d_phases, b)) != cudaSuccess) return fail(HGM_ERR_NOMEM, "plan phases: %s", cudaGetErrorString(e));
+        if ((e = plan_alloc(p, 1, &p->d_phases, b)) != cudaSuccess) return fail(HGM_ERR_NOMEM, "plan phases: %s", cudaGetErrorString(e));
         if ((e = cudaMemcpy(p->d_phases, p->phases.data(), b, cudaMemcpyHostToDevice)) != cudaSuccess)
             return fail(HGM_ERR_CUDA, "plan phases copy: %s", cudaGetErrorString(e));
     }
@@ -273,13 +280,13 @@ int upload_plan(Plan *p) {
             }
         }
         const size_t b = tab.size() * sizeof(uint32_t);
-        if ((e = cudaMalloc(&p->d_layouts, b)) != cudaSuccess)
+        if ((e = plan_alloc(p, 2, &p->d_layouts, b)) != cudaSuccess)
             return fail(HGM_ERR_NOMEM, "plan layouts: %s", cudaGetErrorString(e));
         if ((e = cudaMemcpy(p->d_layouts, tab.data(), b, cudaMemcpyHostToDevice)) != cudaSuccess)
             return fail(HGM_ERR_CUDA, "plan layouts copy: %s", cudaGetErrorString(e));
     }
     if (p->renorm_every > 0) {
-        if ((e = cudaMalloc(&p->d_norm, 64 * sizeof(double))) != cudaSuccess)
+        if ((e = plan_alloc(p, 3, (void **)&p->d_norm, 64 * sizeof(double))) != cudaSuccess)
             return fail(HGM_ERR_NOMEM, "plan norm slots: %s", cudaGetErrorString(e));
     }
     for (PassArgs &pa : p->passes) {

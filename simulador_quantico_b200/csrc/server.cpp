@@ -72,7 +72,7 @@ struct Request {
 // of the GPU: a long plan (a Grover circuit is thousands of passes) then
 // neither fills the launch queue -- where the worker would block, and every
 // other slot with it -- nor starves the slots admitted after it.
-constexpr int64_t kChunkLaunches = 32;
+constexpr int64_t kChunkLaunches = 16;
 
 struct Slot {
     cudaStream_t stream = nullptr;
@@ -141,7 +141,46 @@ struct StateCache {
     }
 };
 
+// Device memory for the plans the planner threads upload, recycled by
+// power-of-two size class (a plan's records are a few tens of KB).
+// cudaMalloc and cudaFree take the device's allocation lock and cudaFree
+// can wait on running work, so freeing a finished request's plan while
+// other slots run stalled them all; recycled blocks avoid both calls.
+struct PlanMemory : DevAllocator {
+    std::mutex mu;
+    std::map<size_t, std::vector<void *>> free_by_class;
+    static size_t size_class(size_t b) {
+        size_t c = 256;
+        while (c < b) c <<= 1;
+        return c;
+    }
+    cudaError_t alloc(void **p, size_t bytes) override {
+        const size_t c = size_class(bytes);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            auto &v = free_by_class[c];
+            if (!v.empty()) {
+                *p = v.back();
+                v.pop_back();
+                return cudaSuccess;
+            }
+        }
+        return cudaMalloc(p, c);
+    }
+    // The GPU must be done with the block.
+    void free(void *p, size_t bytes) override {
+        std::lock_guard<std::mutex> lk(mu);
+        free_by_class[size_class(bytes)].push_back(p);
+    }
+    ~PlanMemory() {
+        for (auto &kv : free_by_class)
+            for (void *p : kv.second) cudaFree(p);
+    }
+};
+
 struct Server {
+    // declared first, destroyed last: every plan below returns its blocks here
+    PlanMemory plan_mem;
     hgm_server_opts opts;
     StateCache cache;
     std::mutex mu;
@@ -156,6 +195,8 @@ struct Server {
     std::atomic<bool> stop{false};
     std::thread worker;
     std::deque<Request *> to_plan;   // submitted circuits waiting for a planner thread
+    // plans of finished requests, released by a planner thread
+    std::vector<std::unique_ptr<Plan>> to_reap;
     std::condition_variable plan_cv;
     std::vector<std::thread> planners;
     int planning = 0;                // circuits being planned
@@ -224,6 +265,10 @@ struct Server {
             r->state.d = nullptr;
             std::lock_guard<std::mutex> lk(mu);
             bytes_in_use -= r->bytes;
+            if (r->owned) {
+                to_reap.push_back(std::move(r->owned));
+                plan_cv.notify_one();
+            }
             delete r;
         }
         s.req = nullptr;
@@ -291,15 +336,23 @@ struct Server {
         cudaSetDevice(device);
         for (;;) {
             Request *r = nullptr;
+            std::vector<std::unique_ptr<Plan>> reap;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                while (!stop && to_plan.empty()) plan_cv.wait_for(lk, std::chrono::milliseconds(100));
+                while (!stop && to_plan.empty() && to_reap.empty())
+                    plan_cv.wait_for(lk, std::chrono::milliseconds(100));
                 if (stop) return;
-                r = to_plan.front();
-                to_plan.pop_front();
-                planning++;
+                reap.swap(to_reap);
+                if (!to_plan.empty()) {
+                    r = to_plan.front();
+                    to_plan.pop_front();
+                    planning++;
+                }
             }
+            reap.clear();  // returns the finished requests' plan memory
+            if (!r) continue;
             r->owned.reset(new Plan());
+            r->owned->allocator = &plan_mem;
             int rc = build_plan(r->ops, r->n, r->popts, r->owned.get());
             if (!rc) rc = upload_plan(r->owned.get());
             std::vector<Op>().swap(r->ops);
