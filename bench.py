@@ -44,6 +44,9 @@ from pathlib import Path
 
 import numpy as np
 
+# one hardware queue per server slot (16 streams); set before any CUDA context
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 

@@ -45,7 +45,10 @@ typedef struct hgm_state hgm_state;
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *hgm_last_error(void);
-/* Initialises the CUDA context on `device` (setDevice, src/core/kernel.cu:31-33). */
+/* Initialises the CUDA context on `device` (setDevice, src/core/kernel.cu:31-33).
+ * Sets CUDA_DEVICE_MAX_CONNECTIONS=32 first unless the environment has it
+ * (one hardware queue per server slot; effective only before the process
+ * creates its CUDA context). */
 int hgm_init(int device);
 /* Blocks until all work queued by this library has finished. */
 int hgm_synchronize(void);

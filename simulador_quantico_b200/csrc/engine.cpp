@@ -2,6 +2,8 @@
 // device-resident measurement (include/hgm_b200.h).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -36,6 +38,12 @@ void ops_from_ref_pts(void *const *pts, std::vector<Op> &out) {
 extern "C" {
 
 int hgm_init(int device) {
+    // The server runs up to 16 streams; with the driver's default of 8
+    // hardware queues, two streams share a queue and a long pass on one holds
+    // back the other's kernels (served throughput swung between 183 and 264
+    // circuits/s with 8, held at 266-268 with 32).  Takes effect only if no
+    // CUDA context exists yet in this process; a value the user set stays.
+    setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     e = cudaFree(0);
