@@ -231,14 +231,45 @@ __device__ __forceinline__ void reg_dense(A2 (&a)[1 << R], const Real (&m)[8], u
     }
 }
 
+// FP32 real 2x2 on packed (re, im) pairs: one f32x2 multiply and one f32x2
+// fused multiply-add per output amplitude instead of two of each (the same
+// IEEE operations per component, so the results are bit-identical); the
+// coefficients come in duplicated, (m, m), built once per gate.
+__device__ __forceinline__ void ip_real_x2(float &xr, float &xi, float &yr, float &yi, unsigned long long c00,
+                                           unsigned long long c01, unsigned long long c10, unsigned long long c11) {
+    asm("{\n\t.reg .b64 X, Y, P, Q;\n\t"
+        "mov.b64 X, {%0, %1};\n\tmov.b64 Y, {%2, %3};\n\t"
+        "mul.rn.f32x2 P, %4, X;\n\tmul.rn.f32x2 Q, %6, X;\n\t"
+        "fma.rn.f32x2 P, %5, Y, P;\n\tfma.rn.f32x2 Q, %7, Y, Q;\n\t"
+        "mov.b64 {%0, %1}, P;\n\tmov.b64 {%2, %3}, Q;\n\t}"
+        : "+f"(xr), "+f"(xi), "+f"(yr), "+f"(yi)
+        : "l"(c00), "l"(c01), "l"(c10), "l"(c11));
+}
+__device__ __forceinline__ unsigned long long dup_f32(float v) {
+    unsigned long long d;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(d) : "f"(v));
+    return d;
+}
+
 template <typename Real, typename A2, int R, int T, bool CTRL>
 __device__ __forceinline__ void reg_real(A2 (&a)[1 << R], const Real (&m)[8], uint32_t cm, uint32_t cv) {
+    if constexpr (sizeof(Real) == 4) {
+        const unsigned long long c00 = dup_f32(m[0]), c01 = dup_f32(m[2]), c10 = dup_f32(m[4]), c11 = dup_f32(m[6]);
 #pragma unroll
-    for (int r = 0; r < (1 << R); r++) {
-        if (r & (1 << T)) continue;
-        const int r1 = r | (1 << T);
-        HGM_PAIR_GUARD(r)
-        ip_real(a[r].x, a[r].y, a[r1].x, a[r1].y, m[0], m[2], m[4], m[6]);
+        for (int r = 0; r < (1 << R); r++) {
+            if (r & (1 << T)) continue;
+            const int r1 = r | (1 << T);
+            HGM_PAIR_GUARD(r)
+            ip_real_x2(a[r].x, a[r].y, a[r1].x, a[r1].y, c00, c01, c10, c11);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) {
+            if (r & (1 << T)) continue;
+            const int r1 = r | (1 << T);
+            HGM_PAIR_GUARD(r)
+            ip_real(a[r].x, a[r].y, a[r1].x, a[r1].y, m[0], m[2], m[4], m[6]);
+        }
     }
 }
 
