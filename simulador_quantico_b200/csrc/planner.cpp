@@ -167,12 +167,16 @@ struct LayoutMaker {
         }
         return lay;
     }
-    // Adds bits to S until it has R: `first` in order, then bits at or above
-    // L, then any, each only if S stays feasible.
+    // Adds bits to S until it has R, each only if S stays feasible: bits of
+    // `first` at or above L, then any bits at or above L, then `first`'s low
+    // bits, then any (low bits last keep the layout coalesced).
     uint32_t fill(uint32_t S, uint32_t first) const {
-        for (int pass = 0; pass < 3 && __builtin_popcount(S) < R; pass++) {
+        for (int pass = 0; pass < 4 && __builtin_popcount(S) < R; pass++) {
             for (int q = 0; q < K && __builtin_popcount(S) < R; q++) {
-                const bool want = pass == 0 ? ((first >> q) & 1) : pass == 1 ? q >= L : true;
+                const bool want = pass == 0   ? (((first >> q) & 1) && q >= L)
+                                  : pass == 1 ? q >= L
+                                  : pass == 2 ? ((first >> q) & 1)
+                                              : true;
                 if (want && !((S >> q) & 1) && feasible(S | (1u << q))) S |= 1u << q;
             }
         }
@@ -565,22 +569,30 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
             }
             return count;
         };
-        auto first_fit = [&](uint32_t prefer) {
+        // low_first: a first walk lets only gates on the low index bits
+        // (local 0..L-1) claim register bits, so that a phase needing them
+        // comes while later phases can still end the pass in a coalesced
+        // layout (a low-bit phase left last costs a store transpose)
+        auto first_fit = [&](uint32_t prefer, bool low_first) {
             uint32_t S = 0;
-            uint64_t bn = 0, bd = 0;
-            for (int idx : pending) {
-                const SOp &op = ops[idx];
-                bool ok = !conflicts(op, bn, bd);
-                if (ok && op.mc != MC_DIAG) {
-                    const uint32_t b = 1u << loc_of[op.target];
-                    if (!(S & b)) {
-                        if (__builtin_popcount(S) < R && lm.feasible(S | b)) S |= b;
-                        else ok = false;
+            for (int round = low_first ? 0 : 1; round < 2; round++) {
+                uint64_t bn = 0, bd = 0;
+                for (int idx : pending) {
+                    const SOp &op = ops[idx];
+                    bool ok = !conflicts(op, bn, bd);
+                    if (ok && op.mc != MC_DIAG) {
+                        const int l = loc_of[op.target];
+                        const uint32_t b = 1u << l;
+                        if (!(S & b)) {
+                            if (round == 0 && l >= L) ok = false;
+                            else if (__builtin_popcount(S) < R && lm.feasible(S | b)) S |= b;
+                            else ok = false;
+                        }
                     }
-                }
-                if (!ok) {
-                    bn |= op.nd();
-                    bd |= op.dg();
+                    if (!ok) {
+                        bn |= op.nd();
+                        bd |= op.dg();
+                    }
                 }
             }
             return lm.fill(S, prefer);
@@ -588,7 +600,7 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
         while (!pending.empty()) {
             const uint32_t cur_S = cur >= 0 ? LayoutMaker::regs(plan->layouts[cur], R, W) : 0;
             const int count_cur = cur >= 0 ? walk(cur_S, nullptr, nullptr) : -1;
-            const uint32_t S_new = first_fit(cur_S);
+            const uint32_t S_new = first_fit(cur_S, cur >= 0);
             const int count_new = walk(S_new, nullptr, nullptr);
             int lay = cur;
             uint32_t S = cur_S;
