@@ -125,3 +125,15 @@ def test_shor_out_unchanged(sq, prec):
             found += 1
             break
     assert found >= 1
+
+
+def test_wrapper_interleaved_sizes(sq):
+    """The drop-in keeps one device state per qubit count between calls;
+    calls that alternate between sizes still get exact results."""
+    for i, n in enumerate([12, 14, 12, 16, 14, 12]):
+        spec = random_gate_circuit_spec(n, 4 * n, seed=300 + i)
+        init = random_state(n, seed=500 + i)
+        got = run_wrapper(sq, spec, "f64", init)
+        c = spec.build(__import__("oracle.circuit_lang", fromlist=["Circuit"]).Circuit())
+        want = cpu.run_serial(init, n, c.as_arrays())
+        assert np.abs(got - want).max() < TOL_F64, n

@@ -158,3 +158,21 @@ def test_staged_copy_round_trip(sq, prec, n):
     back = st.download()
     st.free()
     assert np.array_equal(back.view(np.uint8), amp.view(np.uint8))
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_plan_freed_right_after_queueing(sq, prec):
+    """A plan dropped as soon as the execution that uses it is queued (a
+    temporary in Python) is freed only after the device finishes with it."""
+    n = 20
+    spec = random_gate_circuit_spec(n, 120, seed=3)
+    init = random_state(n, seed=8)
+    st = sq.State(n, prec).upload(init)
+    for _ in range(3):
+        st.execute(sq.Plan(spec.build(sq.Circuit()), n, prec))  # the plan is freed on return
+    got = st.download()
+    st.free()
+    want = init
+    for _ in range(3):
+        want = oracle_state(spec, "f64", init=want)
+    assert np.abs(got - want.astype(got.dtype)).max() < 10 * TOL[prec]

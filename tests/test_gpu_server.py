@@ -125,3 +125,30 @@ def test_submit_plan_matches_submit(sq):
     with pytest.raises(sq.HgmError):
         srv.submit_plan(sq.Plan(reqs[0][0].build(sq.Circuit()), reqs[0][0].qubits, "f64"))
     srv.close()
+
+
+def test_state_buffers_recycled_within_budget(sq):
+    """Finished states' buffers are reused by later requests of the same
+    size, and cached buffers of other sizes are evicted when a new size would
+    not fit the budget; every result is still exact (each request
+    re-initialises the buffer it gets) and admission stays within budget."""
+    budget = 3 * (8 << 16)  # three 16-qubit FP32 states
+    srv = sq.Server("f32", budget_bytes=budget, max_inflight=4)
+    sizes = [16, 15, 16, 14, 16, 15, 13, 16, 14, 15, 16, 12] * 2
+    ids = {}
+    for i, n in enumerate(sizes):
+        spec = wl.grover_search(n, (37 * i + 5) % (1 << n), iterations=3) if i % 2 else wl.qft(n, (91 * i) % (1 << n))
+        ids[srv.submit(spec.build(sq.Circuit()), n, spec.init_index, (1 << n) - 1)] = spec
+        p = srv.pending()
+        assert p["bytes_in_use"] <= budget
+    results = srv.drain(len(sizes))
+    assert all(r["status"] == 0 for r in results)
+    for r in results:
+        spec = ids[r["id"]]
+        assert abs(r["norm"] - 1.0) < 1e-4
+        if spec.name == "qft":
+            assert abs(r["pmax"] - 2.0 ** -spec.qubits) < 1e-6
+        else:
+            want = oracle_state(spec, "f64")
+            assert r["argmax"] == int(np.argmax(np.abs(want) ** 2))
+    srv.close()
