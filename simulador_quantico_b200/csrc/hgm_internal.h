@@ -90,6 +90,12 @@ constexpr int PB_TERMS = 255;
 // Phase-block head: cv_reg bit b (b < R) marks register bit b as having
 // G/H/D terms; this bit marks F terms.
 constexpr uint32_t PB_F_ACTIVE = 1u << 16;
+// Phase-block head flags (cm_reg): a 2^R table follows the terms; the terms
+// are compact phase terms (PhaseTerm, several per record) and m[] bytes
+// 16..23 hold the index bit of each thread bit (lanes 0..4, warps 5..7).
+constexpr uint32_t PB_HAS_TABLE = 1u;
+constexpr uint32_t PB_ANGLES = 2u;
+
 
 // Target location codes inside a phase: 0..R-1 register bit, 8+q thread bit q
 // (lane bits 0..4, warp bits 5..), 64+g a non-tile index bit g.
@@ -106,6 +112,22 @@ struct alignas(16) DevOp {
     uint64_t cm_glob, cv_glob; // controls on non-tile index bits
     Real m[8];
 };
+
+// A phase-block term whose diagonal entries are pure phases: where its
+// control holds (index bit cbit == cval; cbit < 0: no control), it adds a0
+// or a1 turns (arguments / 2pi of d0, d1) to the phase of its category, by
+// the value of index bit tbit (tbit < 0: a D term, whose category's
+// register bit decides).
+template <typename Real>
+struct PhaseTerm {
+    int8_t cbit, cval, tbit;
+    int8_t pad[sizeof(Real) - 3];
+    Real a0, a1, pad2;
+};
+template <typename Real>
+constexpr int pb_terms_per_record() {
+    return (int)(sizeof(DevOp<Real>) / sizeof(PhaseTerm<Real>));
+}
 
 struct DevPhase {
     int32_t layout;          // index into the plan's layout table

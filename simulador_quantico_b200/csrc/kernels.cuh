@@ -592,6 +592,152 @@ struct PhaseBits<Real, A2, R, R> {
                                                uint32_t, A2 &, uint64_t, uint32_t, uint32_t) {}
 };
 
+// ---- phase blocks of compact phase terms (head flag PB_ANGLES) ------------
+// Each term adds a0 or a1 turns to its category's phase where its control
+// holds; the index bits it tests are those of the thread's register-0
+// amplitude, ix = tile base | the thread bits placed at their index bits
+// (head bytes 16..23).  A category's factor is exp(2 pi i * turns), one
+// sincospi per category instead of a complex multiply per term.
+template <typename Real>
+struct TermWords;
+template <>
+struct TermWords<float> {
+    uint32_t head;
+    float a0, a1;
+    __device__ __forceinline__ TermWords(const unsigned char *p) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p));
+        head = v.x;
+        a0 = __uint_as_float(v.y);
+        a1 = __uint_as_float(v.z);
+    }
+};
+template <>
+struct TermWords<double> {
+    uint32_t head;
+    double a0, a1;
+    __device__ __forceinline__ TermWords(const unsigned char *p) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p));
+        const double2 w = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+        head = v.x;
+        a0 = __hiloint2double((int)v.w, (int)v.z);
+        a1 = w.x;
+    }
+};
+
+// Term k of the block whose terms start at rec0; c: its control holds, tv:
+// the value of its target bit (0 for a D term).
+template <typename Real>
+__device__ __forceinline__ TermWords<Real> phase_term(const unsigned char *__restrict__ rec0, int k, uint64_t ix,
+                                                      bool &c, uint32_t &tv) {
+    constexpr int per = pb_terms_per_record<Real>();
+    const TermWords<Real> t(rec0 + (k / per) * sizeof(DevOp<Real>) + (k % per) * sizeof(PhaseTerm<Real>));
+    const int cbit = (int)(int8_t)(t.head & 0xffu), cval = (int)((t.head >> 8) & 0xffu);
+    const int tbit = (int)(int8_t)((t.head >> 16) & 0xffu);
+    c = cbit < 0 || (int)((ix >> (cbit & 63)) & 1u) == cval;
+    tv = tbit < 0 ? 0u : (uint32_t)((ix >> (tbit & 63)) & 1u);
+    return t;
+}
+
+template <typename Real>
+__device__ __forceinline__ Real turns_sum(const unsigned char *__restrict__ rec0, int k0, int n, uint64_t ix, Real acc) {
+    Real acc2 = 0;
+    int k = 0;
+#pragma unroll 1
+    for (; k + 1 < n; k += 2) {
+        bool ca, cb;
+        uint32_t ta, tb;
+        const TermWords<Real> x = phase_term<Real>(rec0, k0 + k, ix, ca, ta);
+        const TermWords<Real> y = phase_term<Real>(rec0, k0 + k + 1, ix, cb, tb);
+        acc += ca ? (ta ? x.a1 : x.a0) : (Real)0;
+        acc2 += cb ? (tb ? y.a1 : y.a0) : (Real)0;
+    }
+    if (k < n) {
+        bool ca;
+        uint32_t ta;
+        const TermWords<Real> x = phase_term<Real>(rec0, k0 + k, ix, ca, ta);
+        acc += ca ? (ta ? x.a1 : x.a0) : (Real)0;
+    }
+    return acc + acc2;
+}
+
+template <typename A2, typename Real>
+__device__ __forceinline__ A2 cis_turns(Real t) {
+    const Real r = t - rint(t);
+    A2 f;
+    if constexpr (sizeof(Real) == 4) sincospif(2.0f * r, &f.y, &f.x);
+    else sincospi(2.0 * r, &f.y, &f.x);
+    return f;
+}
+
+template <typename Real, typename A2, int R, int B>
+struct PhaseBitsAngles {
+    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const unsigned char *__restrict__ rec0, int k,
+                                               const uint4 &cnt, uint32_t act, Real &carry, uint64_t ix, uint32_t xr) {
+        const int ng = count_byte<1 + B>(cnt), nh = count_byte<1 + R + B>(cnt), nd = count_byte<1 + 2 * R + B>(cnt);
+        if (act & (1u << B)) {
+            Real g = turns_sum<Real>(rec0, k, ng, ix, carry);
+            Real h = turns_sum<Real>(rec0, k + ng, nh, ix, carry);
+            carry = 0;
+#pragma unroll 1
+            for (int i = 0; i < nd; i++) {
+                bool c;
+                uint32_t tv;
+                const TermWords<Real> t = phase_term<Real>(rec0, k + ng + nh + i, ix, c, tv);
+                h += c ? t.a0 : (Real)0;
+                g += c ? t.a1 : (Real)0;
+            }
+            // g belongs to the registers whose label has bit B set
+            const bool flip = (xr >> B) & 1u;
+            const A2 gf = cis_turns<A2>(g), hf = cis_turns<A2>(h);
+            const A2 g1 = flip ? hf : gf, h1 = flip ? gf : hf;
+#pragma unroll
+            for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], ((r >> B) & 1) ? g1 : h1);
+        }
+        PhaseBitsAngles<Real, A2, R, B + 1>::run(a, rec0, k + ng + nh + nd, cnt, act, carry, ix, xr);
+    }
+};
+template <typename Real, typename A2, int R>
+struct PhaseBitsAngles<Real, A2, R, R> {
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const unsigned char *__restrict__, int, const uint4 &,
+                                               uint32_t, Real &, uint64_t, uint32_t) {}
+};
+
+template <typename Real, typename A2, int R>
+__device__ __forceinline__ void apply_phase_block_angles(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op,
+                                                         uint64_t base, uint32_t thr, uint32_t xr) {
+    const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));
+    const int nrec = (int)hdr.y;
+    const bool has_table = hdr.z & PB_HAS_TABLE;
+    const uint32_t act = hdr.w;
+    const uint4 cnt = __ldg(reinterpret_cast<const uint4 *>(op->m));
+    const uint2 tg = __ldg(reinterpret_cast<const uint2 *>(reinterpret_cast<const unsigned char *>(op->m) + 16));
+    uint64_t ix = base;
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+        const uint32_t g = ((t < 4 ? tg.x : tg.y) >> (8 * (t & 3))) & 63u;
+        ix |= (uint64_t)((thr >> t) & 1u) << g;
+    }
+    const unsigned char *rec0 = reinterpret_cast<const unsigned char *>(op + 1);
+    const int nf = count_byte<0>(cnt);
+    Real carry = turns_sum<Real>(rec0, 0, nf, ix, (Real)0);
+    PhaseBitsAngles<Real, A2, R, 0>::run(a, rec0, nf, cnt, act, carry, ix, xr);
+    if ((act & PB_F_ACTIVE) && !(act & ((1u << R) - 1u))) {
+        const A2 f = cis_turns<A2>(carry);
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], f);
+    }
+    if (has_table) {
+        const DevOp<Real> *__restrict__ t = op + 1 + nrec - (1 << R) / 4;
+        const Real *__restrict__ z = t->m;
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) {
+            const uint32_t l = r ^ xr;
+            const A2 f = load_c<Real, A2>(z + (l >> 2) * (sizeof(DevOp<Real>) / sizeof(Real)) + 2 * (l & 3));
+            ip_cmul2(a[r], f);
+        }
+    }
+}
+
 // K_PHASE_BLOCK: the F terms fold into one per-thread factor; each active
 // register bit costs one sweep of the registers (PhaseBits); the F factor
 // rides on the first active bit's sweep, or gets a sweep of its own when no
@@ -653,7 +799,8 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
                                          uint64_t base, uint32_t thr, uint32_t &xr) {
     const int kind = (int)hdr.x, tpos = (int)hdr.y;  // hdr: kind, tpos, cm_reg, cv_reg of `op`
     if (kind == K_PHASE_BLOCK) {
-        apply_phase_block<Real, A2, R>(a, op, base, thr, xr);
+        if (hdr.z & PB_ANGLES) apply_phase_block_angles<Real, A2, R>(a, op, base, thr, xr);
+        else apply_phase_block<Real, A2, R>(a, op, base, thr, xr);
         return;
     }
     if (kind == K_LAYER || kind == K_LAYER_REAL) {

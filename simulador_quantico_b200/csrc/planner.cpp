@@ -18,6 +18,7 @@
 // kernel (kernels.cuh): each phase holds gates whose targets are register
 // bits of its layout, a choice of R of the tile's local bits.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "hgm_internal.h"
@@ -101,6 +102,7 @@ struct Role {
 };
 struct Roles {
     Role of[MAX_LAYOUT_ROLES];
+    int8_t thr_gbit[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // index bit of each thread bit (set by the caller)
     Roles(const Lay &lay, int R, int W) {
         for (int k = 0; k < MAX_LAYOUT_ROLES; k++) of[k] = {ROLE_THREAD, -1};
         for (int k = 0; k < 5 + W + R; k++)
@@ -293,10 +295,16 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
         }
     }
     if ((int)members.size() < min_terms) return false;
+    // compact terms when every term's entries are pure phases
+    bool angles = true;
+    for (const auto &c : cat)
+        for (int idx : c)
+            for (int k : {0, 3})
+                angles = angles && std::abs(std::abs(ops[idx].m[k]) - 1.0) < 1e-12;
     DevOp<Real> head;
     memset(&head, 0, sizeof head);
     head.kind = K_PHASE_BLOCK;
-    head.cm_reg = has_table ? 1u : 0u;
+    head.cm_reg = (has_table ? PB_HAS_TABLE : 0u) | (angles ? PB_ANGLES : 0u);
     uint8_t counts[16] = {0};
     int nrec = 0;
     for (int k = 0; k < 1 + 3 * R; k++) {
@@ -306,14 +314,44 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
         head.cv_reg |= k == 0 ? PB_F_ACTIVE : 1u << ((k - 1) % R);
     }
     const int table_recs = has_table ? (1 << R) / 4 : 0;
+    constexpr int per = pb_terms_per_record<Real>();
+    if (angles) nrec = (nrec + per - 1) / per;
     head.tpos = nrec + table_recs;
     memcpy(head.m, counts, 16);
+    if (angles) memcpy(reinterpret_cast<unsigned char *>(head.m) + 16, ro.thr_gbit, 8);
     out.push_back(head);
-    // records in the kernel's walk order: F, then per register bit b: G[b], H[b], D[b]
-    for (int idx : cat[0]) out.push_back(encode<Real>(ops[idx], ro, loc_of, tmask));
+    // terms in the kernel's walk order: F, then per register bit b: G[b], H[b], D[b]
+    std::vector<int> order(cat[0]);
     for (int b = 0; b < R; b++)
-        for (int k : {1 + b, 1 + R + b, 1 + 2 * R + b})
-            for (int idx : cat[k]) out.push_back(encode<Real>(ops[idx], ro, loc_of, tmask));
+        for (int k : {1 + b, 1 + R + b, 1 + 2 * R + b}) order.insert(order.end(), cat[k].begin(), cat[k].end());
+    if (!angles) {
+        for (int idx : order) out.push_back(encode<Real>(ops[idx], ro, loc_of, tmask));
+    } else {
+        const double turn = 1.0 / (2.0 * 3.14159265358979323846);
+        std::vector<PhaseTerm<Real>> terms;
+        for (int idx : order) {
+            const SOp &op = ops[idx];
+            PhaseTerm<Real> t;
+            memset(&t, 0, sizeof t);
+            const int c_bit = op.cmask ? __builtin_ctzll(op.cmask) : -1;
+            const bool c_reg = c_bit >= 0 && ((tmask >> c_bit) & 1) && ro.of[loc_of[c_bit]].kind == ROLE_REG;
+            const bool t_reg = ((tmask >> op.target) & 1) && ro.of[loc_of[op.target]].kind == ROLE_REG;
+            t.cbit = (int8_t)(c_reg ? -1 : c_bit);  // G/H: the control is the category's register bit
+            t.cval = (int8_t)(c_bit >= 0 ? (op.cval >> c_bit) & 1 : 0);
+            t.tbit = (int8_t)(t_reg ? -1 : op.target);
+            t.a0 = (Real)(std::arg(op.m[0]) * turn);
+            t.a1 = (Real)(std::arg(op.m[3]) * turn);
+            terms.push_back(t);
+        }
+        for (int r = 0; r < nrec; r++) {
+            DevOp<Real> rec;
+            memset(&rec, 0, sizeof rec);
+            for (int j = 0; j < per && r * per + j < (int)terms.size(); j++)
+                memcpy(reinterpret_cast<unsigned char *>(&rec) + j * sizeof(PhaseTerm<Real>), &terms[r * per + j],
+                       sizeof(PhaseTerm<Real>));
+            out.push_back(rec);
+        }
+    }
     for (int q = 0; q < table_recs; q++) {
         DevOp<Real> rec;
         memset(&rec, 0, sizeof rec);
@@ -615,7 +653,9 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
             DevPhase ph;
             ph.layout = lay;
             ph.op_begin = (int)dev_ops.size();
-            emit_phase<Real>(ops, taken, Roles(plan->layouts[lay], R, W), R, loc_of, tmask, dev_ops);
+            Roles ro(plan->layouts[lay], R, W);
+            for (int t = 0; t < 5 + W; t++) ro.thr_gbit[t] = pa.tb[plan->layouts[lay].pos[t]];
+            emit_phase<Real>(ops, taken, ro, R, loc_of, tmask, dev_ops);
             ph.op_end = (int)dev_ops.size();
             ph.xwarp = 0;
             if (cur >= 0 && cur != lay) {

@@ -162,7 +162,75 @@ def _term_factor(t, base, thr):
     return ok, f0, d1
 
 
-def apply_phase_block(tile, recs, i, R, base, thr, reg, T, K):
+def phase_terms(recs, first, count, real):
+    """The compact phase terms (struct PhaseTerm) packed in records first.. :
+    a list of (cbit, cval, tbit, a0, a1)."""
+    size = 16 if real == "<f4" else 32
+    per = recs.dtype.itemsize // size
+    tdt = np.dtype([("cbit", "i1"), ("cval", "i1"), ("tbit", "i1"), ("pad", "i1", size // 4 - 3),
+                    ("a0", real), ("a1", real), ("pad2", real)])
+    out = []
+    for k in range(count):
+        raw = recs[first + k // per].tobytes()[(k % per) * size:(k % per + 1) * size]
+        t = np.frombuffer(raw, tdt)[0]
+        out.append((int(t["cbit"]), int(t["cval"]), int(t["tbit"]), float(t["a0"]), float(t["a1"])))
+    return out
+
+
+def apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real):
+    """A phase block of compact phase terms (head flag PB_ANGLES): phases add
+    up in turns per category; the kernel folds F into the first active bit."""
+    head = recs[i]
+    counts = np.frombuffer(head["m"].tobytes()[:16], dtype=np.uint8)
+    tgb = np.frombuffer(head["m"].tobytes()[16:24], dtype=np.int8)
+    has_table = int(head["cm_reg"]) & 1
+    act = int(head["cv_reg"])
+    nrec = int(head["tpos"])
+    ix = base[:, None] | np.zeros((1, 1 << K), dtype=np.int64)
+    for t in range(8):
+        ix = ix | (((thr >> t) & 1).astype(np.int64) << int(tgb[t]))[None, :]
+    terms = phase_terms(recs, i + 1, int(sum(int(c) for c in counts)), real)
+    phase = np.zeros((T, 1 << K))
+
+    def contrib(term):
+        cbit, cval, tbit, a0, a1 = term
+        c = np.ones(ix.shape, bool) if cbit < 0 else (((ix >> cbit) & 1) == cval)
+        t = np.zeros(ix.shape, np.int64) if tbit < 0 else ((ix >> tbit) & 1)
+        return c, np.where(t == 1, a1, a0)
+    k = 0
+    for _ in range(int(counts[0])):
+        c, a = contrib(terms[k])
+        if act & PB_F_ACTIVE:
+            phase += np.where(c, a, 0.0)
+        k += 1
+    for b in range(R):
+        bit = ((reg >> b) & 1)[None, :]
+        for kind, cnt in (("G", counts[1 + b]), ("H", counts[1 + R + b]), ("D", counts[1 + 2 * R + b])):
+            for _ in range(int(cnt)):
+                if (act >> b) & 1:
+                    cbit, cval, tbit, a0, a1 = terms[k]
+                    c, a = contrib(terms[k])
+                    if kind == "G":
+                        phase += np.where(c & (bit == 1), a, 0.0)
+                    elif kind == "H":
+                        phase += np.where(c & (bit == 0), a, 0.0)
+                    else:
+                        phase += np.where(c, np.where(bit == 1, a1, a0), 0.0)
+                k += 1
+    f = np.exp(2j * np.pi * phase)
+    if has_table:
+        j = i + 1 + nrec - (1 << R) // 4
+        tab = []
+        for q in range((1 << R) // 4):
+            m = recs[j + q]["m"].astype(np.float64)
+            tab += list(m[0::2] + 1j * m[1::2])
+        f = f * np.asarray(tab)[reg][None, :]
+    return tile * f
+
+
+def apply_phase_block(tile, recs, i, R, base, thr, reg, T, K, real="<f8"):
+    if int(recs[i]["cm_reg"]) & 2:
+        return apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real)
     counts = np.frombuffer(recs[i]["m"].tobytes()[:16], dtype=np.uint8)
     has_table = int(recs[i]["cm_reg"]) & 1
     act = int(recs[i]["cv_reg"])  # active register bits; PB_F_ACTIVE: F terms
@@ -242,7 +310,8 @@ def run(plan, precision, state, iterations=1):
                 while i < len(recs):
                     o = recs[i]
                     if int(o["kind"]) == K_PHASE_BLOCK:
-                        tile = apply_phase_block(tile, recs, i, R, base, thr, reg, T, K)
+                        tile = apply_phase_block(tile, recs, i, R, base, thr, reg, T, K,
+                                                 "<f8" if precision == "f64" else "<f4")
                         i += 1 + int(o["tpos"])
                         continue
                     if int(o["kind"]) in (K_LAYER, K_LAYER_REAL):
