@@ -749,7 +749,7 @@ def workload_served(args, dist, sq):
     steps_reqs = [served_requests(1000 + s, count) for s in range(args.warmup + args.steps)]
     steps_circuits = [[spec.build(sq.Circuit()) for spec, _ in reqs] for reqs in steps_reqs]
     # every request's plan, built and uploaded before any timed region: the device-resident inputs
-    steps_plans = [[sq.Plan(c, spec.qubits, "f32") for (spec, _), c in zip(reqs, cs)]
+    steps_plans = [[sq.Plan(c, spec.qubits, "f32").upload() for (spec, _), c in zip(reqs, cs)]
                    for reqs, cs in zip(steps_reqs, steps_circuits)]
     upload = [sum(p.stats()["upload_bytes"] for p in plans) for plans in steps_plans]
     srv = sq.Server("f32", budget_bytes=150 << 30, max_inflight=args.inflight)

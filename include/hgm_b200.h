@@ -107,6 +107,10 @@ int hgm_plan_create_from_ref_pts(void *const *pts, int pt_precision, int qubits,
 void hgm_plan_free(hgm_plan *p);
 /* Plan statistics: ops after fusion, passes, phases, transposes. */
 int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes);
+/* Copies the plan's device records to the GPU now instead of at its first
+ * execution or submission (so that a timed or latency-critical section does
+ * not pay for the allocation and copy). */
+int hgm_plan_upload(hgm_plan *p);
 
 /* Read-only view of a plan's host-side encoding (for inspection and the
  * CPU emulation test): per-pass kernel arguments (struct PassArgs), register

@@ -66,6 +66,7 @@ def _load():
         "hgm_plan_create_from_ref_pts": ([vp, i, i, P(PlanOpts), P(vp)], i),
         "hgm_plan_free": ([vp], None),
         "hgm_plan_stats": ([vp, P(i64), P(i64), P(i64), P(i64)], i),
+        "hgm_plan_upload": ([vp], i),
         "hgm_plan_export": ([vp, P(vp), P(i64), P(vp), P(i64), P(vp), P(i64), P(i), P(i)], i),
         "hgm_plan_layouts": ([vp, P(vp), P(i64)], i),
         "hgm_state_create": ([i, i, P(vp)], i),

@@ -118,6 +118,11 @@ void hgm_plan_free(hgm_plan *p) {
     delete pl;
 }
 
+int hgm_plan_upload(hgm_plan *p) {
+    if (!p) return fail(HGM_ERR_INVALID, "null plan");
+    return upload_plan(reinterpret_cast<Plan *>(p));
+}
+
 int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes) {
     if (!p) return fail(HGM_ERR_INVALID, "null plan");
     const Plan *pl = reinterpret_cast<const Plan *>(p);

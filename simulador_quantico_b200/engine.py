@@ -116,6 +116,11 @@ class Plan:
             lib.hgm_plan_free(self.h)
             self.h = None
 
+    def upload(self):
+        """Copy the plan's device records now rather than at first use."""
+        check(lib.hgm_plan_upload(self.h))
+        return self
+
     def stats(self) -> dict:
         v = [C.c_int64() for _ in range(4)]
         check(lib.hgm_plan_stats(self.h, *[C.byref(x) for x in v]))
