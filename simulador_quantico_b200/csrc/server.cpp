@@ -12,16 +12,20 @@
 //     device buffers, initialises it, queues the plan's passes, an FP64 norm
 //     and (if asked) the marginal argmax, copies those few numbers to pinned
 //     host memory and records an event;
-//   * polls the slots' events; a finished request records its completion
-//     time, returns (or keeps) its state buffer and frees the slot for the
-//     next one.
+//   * feeds each slot's passes in chunks (at most two chunks ahead of the
+//     GPU) and polls the slots' events; a finished request records its
+//     completion time, returns (or keeps) its state buffer, hands its plan
+//     to a planner thread for release and frees the slot for the next one.
 // State sizes are powers of two, so finished states are kept by size and
 // handed to the next request of that size: after warm-up the worker makes
 // no allocation calls.  (Allocating from the stream-ordered pool per request
 // blocked the worker, and with it every slot, for up to half a second when
 // the pool had to map memory for a 1-2 GiB state.)  New buffers are
 // cudaMalloc'ed while admitted plus cached bytes stay within the budget;
-// cached buffers of other sizes are freed first when they would not.
+// cached buffers of other sizes are freed first when they would not.  Plans
+// the planner threads build take their device memory from a cache of
+// power-of-two blocks (PlanMemory), so serving from host circuits makes no
+// allocation calls once warm either.
 // Requests on different slots run concurrently on the device; new requests
 // are admitted while earlier ones are still executing.  A request's result
 // does not depend on what else runs: it uses its own plan, state and scratch
