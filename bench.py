@@ -960,8 +960,9 @@ def reference_arm(args, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 20 for served, whose 48-request steps last ~0.2 s; else 5)")
+    ap.add_argument("--warmup", type=int, default=None, help="untimed warm-up steps (default 5 served, else 3)")
     ap.add_argument("--workload", default="served", choices=sorted(WORKLOADS))
     ap.add_argument("--requests", type=int, default=0, help="requests per served step (default 48)")
     ap.add_argument("--rate", type=float, default=0.0, help="Poisson arrival rate in requests/s (0: all at once)")
@@ -976,6 +977,10 @@ def main():
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.workload == "served" else 5
+    if args.warmup is None:
+        args.warmup = 5 if args.workload == "served" else 3
     args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
                         "grover": "Grover iterations/s (26q FP64, marked index 42)",
                         "hadamard": "gate-layers/s (H on every qubit, 30q FP64)",
