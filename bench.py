@@ -245,6 +245,11 @@ def e2e_layered(dist, sq, spec, n, prec):
     pts = c.ref_pts(prec)
     host = np.zeros(1 << n, dtype=np.complex64 if prec == "f32" else np.complex128)
     host[0] = 1.0
+    # one untimed call first (device state, staging buffers, host pages), as a
+    # DGM user's repeated execute calls would have
+    L.GpuExecutionWrapper(host.ctypes.data, pts, n, 4, 8, 1, 64, 2, 1)
+    host[:] = 0
+    host[0] = 1.0
     t0 = time.perf_counter()
     L.GpuExecutionWrapper(host.ctypes.data, pts, n, 4, 8, 1, 64, 2, 1)
     dt = time.perf_counter() - t0
@@ -350,6 +355,9 @@ def e2e_hadamard(dist, sq, c, n):
     L.setDevice(dist.local_rank)
     pts = c.ref_pts("f64")
     host = np.zeros(1 << n, dtype=np.complex128)
+    host[0] = 1.0
+    L.GpuExecutionWrapper(host.ctypes.data, pts, n, 4, 8, 1, 64, 2, 1)  # untimed first call
+    host[:] = 0
     host[0] = 1.0
     t0 = time.perf_counter()
     L.GpuExecutionWrapper(host.ctypes.data, pts, n, 4, 8, 1, 64, 2, 1)
