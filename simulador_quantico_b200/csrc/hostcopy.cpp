@@ -7,8 +7,9 @@
 // buffer chunk by chunk between host memory and a chunk (memcpy) and between
 // the chunk and the device (cudaMemcpyAsync), with the two chunks taking
 // turns, so the host copies, the page faults of first-touch host memory and
-// the DMA all run in parallel (27 GB/s host->device with four threads, the
-// fastest count measured; more threads contend).  Registering the caller's
+// the DMA all run in parallel (27-45 GB/s host->device and 42 GB/s
+// device->host with four threads, the fastest count measured; more threads
+// contend).  Registering the caller's
 // buffer instead (cudaHostRegister) copies at 55 GB/s but registering and
 // unregistering 16 GiB takes 2.8 s, more than the copy itself.
 //
