@@ -48,6 +48,26 @@ def test_emulated_workloads(builder):
     assert np.abs(emu.run(plan, "f64", init) - oracle_state(spec, "f64")).max() < 1e-12
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("low_bits,warp_bits", [(3, 0), (4, 3), (5, 1), (4, 2)])
+def test_emulated_tile_settings(prec, low_bits, warp_bits):
+    """The batched autotuner's settings (always-resident low bits 3..5, warp
+    bits 0..3): every layout keeps its conflict-free and coalescing rules
+    (checked inside the emulator) and the plan reproduces the oracle, for a
+    random-gate circuit and for a QFT (compact phase terms)."""
+    n = 15
+    tol = 1e-12 if prec == "f64" else 2e-5
+    for spec in (random_gate_circuit_spec(n, 70, seed=low_bits * 10 + warp_bits), wl.qft(n, 4321)):
+        plan = sq.Plan(spec.build(sq.Circuit()), n, prec, low_bits=low_bits, warp_bits=warp_bits, renorm_every=0)
+        if spec.name == "qft":
+            init = np.zeros(1 << n, dtype=np.complex128)
+            init[spec.init_index] = 1
+        else:
+            init = random_state(n, seed=3)
+        got = emu.run(plan, prec, init)
+        assert np.abs(got - oracle_state(spec, "f64", init=init)).max() < tol, spec.name
+
+
 def test_emulated_fp32_encoding():
     n = 12
     spec = random_gate_circuit_spec(n, 50, seed=9)
