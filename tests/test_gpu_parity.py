@@ -160,6 +160,19 @@ def test_qft_closed_form(sq, n):
     assert fidelity_gap(got32, got) < 1e-6
 
 
+@pytest.mark.parametrize("n,warp_bits", [(18, 0), (18, 3), (22, 2)])
+def test_qft_phase_terms_across_passes(sq, n, warp_bits):
+    """Larger QFTs: their controlled phases pair tile bits with thread and
+    non-tile bits over several passes, as compact phase terms (FP64 and FP32)."""
+    x = (0x1F3D5 * n) % (1 << n)
+    spec = wl.qft(n, x)
+    want = cf.qft_basis(n, x)
+    got, _ = engine_state(sq, spec, "f64", warp_bits=warp_bits)
+    assert np.abs(got - want).max() < TOL_F64
+    got32, _ = engine_state(sq, spec, "f32", warp_bits=warp_bits)
+    assert fidelity_gap(got32, want) < 1e-6
+
+
 def test_iterations_replay(sq):
     """Applying the PT list `iterations` times equals unrolling it."""
     n = 13
