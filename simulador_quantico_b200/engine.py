@@ -109,7 +109,8 @@ class Plan:
         self.h = C.c_void_p()
         self.precision = PREC[precision]
         self.qubits = qubits
-        check(lib.hgm_plan_create(circuit.h, qubits, C.byref(plan_opts(precision, **kw)), C.byref(self.h)))
+        self.opts = plan_opts(precision, **kw)
+        check(lib.hgm_plan_create(circuit.h, qubits, C.byref(self.opts), C.byref(self.h)))
 
     def __del__(self):
         if getattr(self, "h", None):

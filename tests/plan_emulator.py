@@ -74,7 +74,7 @@ def local_of(pos, R, W, lane, warp, reg):
     return j | sum(((reg >> q) & 1) << int(pos[5 + W + q]) for q in range(R))
 
 
-def check_pass_layouts(e, pa, R, W, K):
+def check_pass_layouts(e, pa, R, W, K, low_bits=3):
     """The kernel's assumptions about a pass's layouts: every layout is a
     permutation of the K local bits; its low thread bits keep the padded
     transposes free of bank conflicts; the load and store layouts move whole
@@ -95,11 +95,10 @@ def check_pass_layouts(e, pa, R, W, K):
     for key, li in (("ld_gbit", int(pa["load_layout"])), ("st_gbit", int(pa["store_layout"]))):
         pos = lays[li]
         assert [int(x) for x in pa[key][:5 + W + R]] == [tb[int(pos[k])] for k in range(5 + W + R)]
-        low = 0
-        while low < K and tb[low] == low:
-            low += 1
-        for t in range(min(low, 3)):
-            assert int(pos[t]) == t, ("uncoalesced", key, pos)
+        # the planner keeps index bits 0..low_bits-1 at local 0..low_bits-1
+        # and puts them on thread bits 0..low_bits-1 of these layouts
+        for t in range(min(low_bits, 5, K)):
+            assert tb[t] == t and int(pos[t]) == t, ("uncoalesced", key, pos)
     cur = int(pa["load_layout"])
 
     def same_warps(a, b):
@@ -279,7 +278,10 @@ def run(plan, precision, state, iterations=1):
     for _ in range(iterations):
         for pa in e["passes"]:
             K = int(pa["k"])
-            check_pass_layouts(e, pa, R, W, K)
+            lb = getattr(getattr(plan, "opts", None), "low_bits", -1)
+            if lb < 0:
+                lb = 3 if precision == "f64" else 4
+            check_pass_layouts(e, pa, R, W, K, lb)
             tb = [int(x) for x in pa["tb"][:K]]
             tmask = int(pa["tile_mask"])
             free = [g for g in range(n) if not (tmask >> g) & 1]
