@@ -120,3 +120,32 @@ def test_grover_plan_fast():
     dt = time.time() - t0
     assert dt < 20.0
     assert p.stats()["passes"] < 6 * 6433
+
+
+def test_randomized_plans():
+    """Seeded random mix of precisions, tile settings, fusion and circuit
+    families: every emulated plan (layout rules checked inside) reproduces
+    the oracle."""
+    rng = np.random.default_rng(20261203)
+    for case in range(40):
+        prec = ["f64", "f32"][case % 2]
+        R = 4 if prec == "f64" else 5
+        n = int(rng.integers(5 + R, 14))
+        W = min(int(rng.integers(0, 4)), n - 5 - R)
+        lb = int(rng.integers(0, 6))
+        kind = case % 4
+        if kind == 0:
+            spec = random_gate_circuit_spec(n, int(rng.integers(5, 6 * n)), seed=int(rng.integers(1 << 30)),
+                                            max_controls=int(rng.integers(0, 4)))
+            init = random_state(n, seed=case)
+        else:
+            spec = [None, lambda: wl.qft(n, int(rng.integers(1 << n))),
+                    lambda: wl.random_layered(n, int(rng.integers(1, 4)), case),
+                    lambda: wl.grover_search(n, int(rng.integers(1 << n)), iterations=2)][kind]()
+            init = np.zeros(1 << n, dtype=np.complex128)
+            init[spec.init_index] = 1
+        plan = sq.Plan(spec.build(sq.Circuit()), n, prec, warp_bits=W, low_bits=lb, fuse=case % 3 != 0,
+                       renorm_every=0)
+        got = emu.run(plan, prec, init)
+        want = oracle_state(spec, "f64", init=init)
+        assert np.abs(got - want).max() < (1e-11 if prec == "f64" else 5e-5), (case, prec, n, W, lb, spec.name)
