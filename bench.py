@@ -2,10 +2,12 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl b200|reference]
 
-Workloads (synthetic, seeded; see DESIGN.md for the shapes):
-  served   the serving stream: a seeded request mix (random layered
-           circuits, QFTs, Grover searches) served by the continuous-batching
-           server in FP32 with FP64 norm checks; metric served circuits/s
+Workloads (synthetic, seeded):
+  served   the serving stream: a seeded request mix (60% random layered
+           circuits of 12-26 qubits, 30% QFTs of 16-28, 10% Grover searches
+           of 14-20) served by the continuous-batching server in FP32 with
+           FP64 norm checks; metric served circuits/s; default 20 timed steps
+           of 48 requests after 5 warm-up steps
   batched  512 circuits of 10-22 qubits (half QFTs, half random layered) in
            one persistent kernel replayed from a CUDA graph, FP32 (value) and
            FP64, autotuned; metric batched circuits/s
