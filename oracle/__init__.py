@@ -1,7 +1,7 @@
 """CPU oracle for the HybriD-GM t_GPU path (test infrastructure only).
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
-leg import this package, and only as the checker.  The product package
+leg import this package, and only to check results against.  The product package
 (simulador_quantico_b200) never imports it.
 
 * circuit_lang   Python restatement of the reference's circuit language.

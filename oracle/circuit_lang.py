@@ -1,7 +1,8 @@
 """Python restatement of the reference's circuit language (test oracle only).
 
 TEST INFRASTRUCTURE: imported by tests/, __graft_entry__.smoke() and
-bench.py's cpu_baseline leg as the checker; the product never imports it.
+bench.py's cpu_baseline leg, to check results against; the product never
+imports it.
 
 Restates, function by function, how the reference turns gate strings into
 the NULL-terminated PT list that every backend consumes:
