@@ -64,6 +64,25 @@ FALLBACK_HBM_GBS = 6650.0
 TRAFFIC_OVER_ALGO = {"f32": 0.947, "f64": 0.975, "f64_hadamard": 0.996}
 
 
+_WL = None
+
+
+def _workloads():
+    """The circuit builders (simulador_quantico_b200/workloads.py), loaded by path: they need only numpy, and
+    the reference arm must not import the engine package, whose import loads the CUDA library."""
+    global _WL
+    if _WL is None:
+        import importlib.util
+
+        name = "hgm_bench_workloads"
+        spec = importlib.util.spec_from_file_location(name, ROOT / "simulador_quantico_b200" / "workloads.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+        _WL = mod
+    return _WL
+
+
 def hbm_peak():
     try:
         p = json.loads(PEAKS_FILE.read_text())
@@ -192,7 +211,7 @@ def run_timed(dist, sq, step, steps, warmup):
 
 
 def workload_layered(args, dist, sq):
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     n, layers, prec = args.qubits or 30, args.layers or 40, args.precision
     spec = wl.random_layered(n, layers, seed=2024)
@@ -218,11 +237,8 @@ def workload_layered(args, dist, sq):
     # end to end through the reference's C-ABI with host buffers (1 step)
     e2e = e2e_layered(dist, sq, spec, n, prec) if not args.skip_e2e else None
     st.free()
-    line = base_line(args, dist, "gate-layers/s (30q random Rz/Ry+CNOT layers)", value, "layers/s", ms_step,
-                     prec, {"workload": f"layered-{n}q-{layers}layers", "qubits": n, "layers": layers,
-                            "precision": {"f64": "fp64", "f32": "fp32"}[prec],
-                            "state_bytes": S, "passes_per_step": stats["passes"], "ops_after_fusion": stats["ops"],
-                            "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"})
+    line = base_line(args, dist, METRICS["layered"], value, "layers/s", ms_step, prec, config_for(args))
+    line["plan"] = {"passes_per_step": stats["passes"], "ops_after_fusion": stats["ops"]}
     line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(achieved / peak, 4),
                         "traffic": round(TRAFFIC_OVER_ALGO[prec] * 2 * S / 1e9, 3), "traffic_unit": "GB per launch",
@@ -265,7 +281,7 @@ def e2e_layered(dist, sq, spec, n, prec):
 def cpu_baseline_layered(args, kind="reference"):
     """t_PAR_CPU on a bounded sample: 2 layers at 26 qubits, scaled by 2^(30-26)."""
     from oracle import cpu
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     n_s, layers_s = 26, 2
     spec = wl.random_layered(n_s, layers_s, seed=2024)
@@ -306,7 +322,7 @@ def cpu_baseline_layered(args, kind="reference"):
 def workload_hadamard(args, dist, sq):
     """H on every qubit of a 30-qubit FP64 state: a gate layer with few gates per pass, so the pass kernel
     is bound by HBM rather than by its FP64 pipe.  One step = the layer."""
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     n = args.qubits or 30
     spec = wl.hadamard_benchmark(n, iterations=1)
@@ -329,10 +345,8 @@ def workload_hadamard(args, dist, sq):
     p0 = st.prob_one(0)
     st.free()
     peak, peak_kind = hbm_peak()
-    line = base_line(args, dist, "gate-layers/s (H on every qubit, 30q FP64)", value, "layers/s", ms_step, "f64",
-                     {"workload": f"hadamard-layer-{n}q-fp64", "qubits": n, "gates_per_layer": n,
-                      "passes_per_step": stats["passes"], "state_bytes": S,
-                      "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"})
+    line = base_line(args, dist, METRICS["hadamard"], value, "layers/s", ms_step, "f64", config_for(args))
+    line["plan"] = {"passes_per_step": stats["passes"]}
     line["check"] = {"layers_applied": runs, "prob_one_bit0": p0,
                      "ok": bool(abs(p0 - (0.5 if runs % 2 else 0.0)) < 1e-9)}
     line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -373,7 +387,7 @@ def e2e_hadamard(dist, sq, c, n):
 def cpu_baseline_hadamard(args, n, n_s=26):
     """t_PAR_CPU: the layer at 26 qubits, scaled by 2^(n-26)."""
     from oracle import cpu
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     threads = os.cpu_count() or 1
     spec = wl.hadamard_benchmark(n_s, iterations=1)
@@ -412,7 +426,7 @@ GROVER_N, GROVER_MARK, GROVER_STEP_ITERS = 26, 42, 64
 def grover_parts(sq, n, mark):
     """The Grover circuit as two plans: H on every qubit, and one iteration
     (phase oracle on |mark>, H^n, sign flip on |0..0>, H^n)."""
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     spec = wl.grover_search(n, mark)
     (h_steps, _, _), (it_steps, _, _) = spec.calls
@@ -450,10 +464,8 @@ def workload_grover(args, dist, sq):
     found, pmax = st.marginal_argmax((1 << n) - 1)
     st.free()
     peak, peak_kind = hbm_peak()
-    line = base_line(args, dist, "Grover iterations/s (26q FP64, marked index 42)", value, "iterations/s", ms_step,
-                     "f64", {"workload": f"grover-{n}q-fp64", "qubits": n, "marked": mark,
-                             "iterations_per_step": step_iters, "passes_per_iteration": stats["passes"],
-                             "state_bytes": S, "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"})
+    line = base_line(args, dist, METRICS["grover"], value, "iterations/s", ms_step, "f64", config_for(args))
+    line["plan"] = {"passes_per_iteration": stats["passes"]}
     line["search"] = {"iterations": total_iters, "argmax": int(found), "probability": round(pmax, 12),
                       "ok": bool(found == mark and pmax > 0.99), "timed_iterations_before_check": done}
     line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -491,7 +503,7 @@ def e2e_grover(dist, sq, c_init, c_one, n, iters):
 def cpu_baseline_grover(args, n, mark, n_s=22, iters=8):
     """t_PAR_CPU on a bounded sample: 8 iterations at 22 qubits, scaled by 2^(n-22)."""
     from oracle import cpu
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     threads = os.cpu_count() or 1
     spec = wl.grover_search(n_s, mark, iterations=iters)
@@ -531,7 +543,7 @@ def cpu_baseline_grover(args, n, mark, n_s=22, iters=8):
 
 def batched_specs(seed, count=512, lo=10, hi=22):
     """Half exact QFTs of random basis inputs, half 10-layer random Rz/Ry+CNOT circuits; qubits uniform."""
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     rng = np.random.default_rng(seed)
     specs = []
@@ -617,13 +629,10 @@ def workload_batched(args, dist, sq):
     with ClockSampler(dist.local_rank) as clk:
         f32 = batched_one(args, dist, sq, specs, circuits, "f32")
     f64 = batched_one(args, dist, sq, specs, circuits, "f64")
-    line = base_line(args, dist, "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
-                     f32["value"], "circuits/s", f32["ms_per_step"], "f32",
-                     {"workload": f"batched-{count}", "circuits": count, "qubits": "uniform 10-22",
-                      "mix": "half QFT of a random basis input, half 10-layer random Rz/Ry+CNOT",
-                      "inputs": "plans and basis indices uploaded before the timed region; a step is one graph "
-                                "replay (state init + every circuit)",
-                      "l2": "arena of all states (~2.6 GB FP32) > 126 MB L2, no flush needed"})
+    line = base_line(args, dist, METRICS["batched"], f32["value"], "circuits/s", f32["ms_per_step"], "f32",
+                     config_for(args))
+    line["inputs"] = ("plans and basis indices uploaded before the timed region; a step is one graph replay "
+                      "(state init + every circuit)")
     line["gpu_launches"] = f32["gpu_launches"]
     line["roofline"] = f32["roofline"]
     line["fp32"] = f32
@@ -638,36 +647,50 @@ def workload_batched(args, dist, sq):
     return line
 
 
-def cpu_baseline_batched(args, specs, n_cap=18):
-    """t_PAR_CPU (FP32) on every 8th circuit, each on at most n_cap qubits, time scaled by 2^(n - n_cap)
-    and by 8 for the circuits not run."""
-    from oracle import circuit_lang as cl
+def ref_run_request(spec, prec, threads):
+    """Runs one circuit on the reference's own engine the way its algorithm libraries do
+    (src/algorithms/lib_general.cpp:30-36, lib_grover.cpp:30-59): a DGM with its state allocated,
+    setMemoryValue, the circuit's gates (Gates::addGate), one setFunction per call of the circuit and one
+    execute on t_PAR_CPU with `threads` OpenMP threads.  Returns the wall seconds of all of it."""
+    from oracle import cpu
+
+    t0 = time.perf_counter()
+    r = cpu.RefDGM(spec.qubits, prec)
+    r.set_memory_value(spec.init_index)
+    spec.build(r)
+    r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
+    r.execute(1)
+    dt = time.perf_counter() - t0
+    r.close()
+    return dt
+
+
+def ref_stream(specs, prec, threads, budget_s, cursor=0):
+    """Runs specs[cursor], specs[cursor+1], ... unscaled on the reference until budget_s seconds have been
+    spent (the request that crosses the budget completes); returns (requests run, seconds, per-request
+    seconds, next cursor).  Wraps around the list."""
+    done, spent, each = 0, 0.0, []
+    while spent < budget_s and specs:
+        dt = ref_run_request(specs[cursor % len(specs)], prec, threads)
+        each.append(dt)
+        spent += dt
+        done += 1
+        cursor += 1
+    return done, spent, each, cursor
+
+
+def cpu_baseline_batched(args, specs, budget_s=20.0):
+    """The reference's t_PAR_CPU (FP32, unmodified) on the batch's circuits in order, each run unscaled and
+    alone, for about budget_s seconds."""
     from oracle import cpu
 
     threads = os.cpu_count() or 1
-    kind = "reference" if cpu.ref_available("f32") else "port"
-    total = 0.0
-    sample = specs[::8]
-    for spec in sample:
-        full = spec.build(cl.Circuit())
-        t, cm, cv, m = full.as_arrays()
-        n = spec.qubits
-        ns = min(n, n_cap)
-        shift = n - ns
-        keep = [i for i in range(len(t)) if t[i] >= shift and (int(cm[i]) >> shift << shift) == int(cm[i])]
-        ops = (t[keep] - shift, cm[keep] >> shift, cv[keep] >> shift, m[keep])
-        s0 = cpu.basis_state(ns, spec.init_index >> shift, np.complex64)
-        if kind == "reference":
-            dt = ref_replay(ns, s0, ops, threads)
-        else:
-            t0 = time.perf_counter()
-            cpu.run_regions(s0, ns, ops, prec="f32", threads=threads)
-            dt = time.perf_counter() - t0
-        total += dt * (1 << shift)
-    total *= len(specs) / len(sample)
-    return {"value": round(len(specs) / total, 6), "unit": "circuits/s", "cores": threads, "kind": kind,
-            "sample": f"every 8th of the {len(specs)} circuits on t_PAR_CPU FP32, each on <= {n_cap} qubits, time "
-                      "scaled by state size and by 8"}
+    if not cpu.ref_available("f32"):
+        return None
+    done, spent, _, _ = ref_stream(specs, "f32", threads, budget_s)
+    return {"value": round(done / spent, 6), "unit": "circuits/s", "cores": threads, "kind": "reference",
+            "sample": f"the first {done} of the {len(specs)} circuits in batch order on t_PAR_CPU FP32, each "
+                      f"unscaled, one setFunction + execute per circuit ({spent:.1f} s)"}
 
 
 # ---------------------------------------------------------------------------
@@ -681,7 +704,7 @@ def served_requests(seed, count, max_qubits=28):
     """The serving mix: 60% random layered (12-26 qubits, depth 20), 30% QFT
     (16-28 qubits) on a random basis input, 10% Grover (14-20 qubits, marked
     index uniform); all drawn from `seed`."""
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     rng = np.random.default_rng(seed)
     reqs = []
@@ -795,13 +818,9 @@ def workload_served(args, dist, sq):
     plain = plain_fp64(sq, steps_reqs[args.warmup], steps_circuits[args.warmup], args.plain_limit) \
         if not args.skip_e2e else None
     peak, peak_kind = hbm_peak()
-    line = base_line(args, dist, SERVED_METRIC, value, "circuits/s", ms_step, "f32",
-                     {"workload": f"served-mix-{count}req", "requests_per_step": count, "rate_hz": args.rate,
-                      "max_inflight": args.inflight, "budget_bytes": 150 << 30, "precision": "fp32 amplitudes, "
-                      "fp64 gate matrices, norms and argmax", "mix": "60% layered 12-26q d20, 30% QFT 16-28q, "
-                      "10% Grover 14-20q", "inputs": "plans built and uploaded before the timed region "
-                      "(hgm_server_submit_plan); states initialised on the device",
-                      "l2": "states up to 2 GiB; no flush (serving keeps states resident)"})
+    line = base_line(args, dist, SERVED_METRIC, value, "circuits/s", ms_step, "f32", config_for(args))
+    line["inputs"] = ("plans built and uploaded before the timed region (hgm_server_submit_plan); states "
+                      "initialised on the device")
     line["latency_ms"] = latency
     line["rate_sweep"] = sweep
     line["fidelity"] = fid
@@ -852,7 +871,7 @@ def plain_fp64(sq, reqs, circuits, limit):
 
 def served_roofline(sq, args, peak, peak_kind):
     """Roofline of the dominant kernel (the FP32 pass kernel) on the mix's largest layered circuit."""
-    from simulador_quantico_b200 import workloads as wl
+    wl = _workloads()
 
     n = 26
     spec = wl.random_layered(n, 20, seed=99)
@@ -876,64 +895,66 @@ def served_roofline(sq, args, peak, peak_kind):
             "algorithmic_bytes_per_launch": 2 * S}
 
 
-def ref_replay(ns, s0, ops, threads):
-    """Replays (target, cmask, cval, matrix) ops on the reference's FP32 t_PAR_CPU engine as single-gate
-    steps from state s0; returns the seconds spent in the engine's execute calls."""
-    from oracle import cpu
-
-    r = cpu.RefDGM(ns, "f32")
-    r.set_state(s0)
-    r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
-    dt = 0.0
-    for i in range(len(ops[0])):
-        name = f"s{i}"
-        r.add_gate(name, ops[3][i])
-        tok = ["ID"] * ns
-        tgt = ns - 1 - int(ops[0][i])
-        cbits = int(ops[1][i])
-        for b in range(ns):
-            if (cbits >> b) & 1:
-                tok[ns - 1 - b] = "Control1(1)" if (int(ops[2][i]) >> b) & 1 else "Control1(0)"
-        tok[tgt] = f"Target1({name})" if cbits else name
-        r.set_function(",".join(tok), 1, True)
-        t0 = time.perf_counter()  # the engine's execution only, not the parse of the step
-        r.execute(1)
-        dt += time.perf_counter() - t0
-    r.close()
-    return dt
-
-
-def cpu_baseline_served(args, reqs, n_cap=20, op_cap=400):
-    """The reference's t_PAR_CPU (FP32, unmodified) on the same request list, each request run on at most
-    n_cap qubits and its first op_cap gates, the time scaled by 2^(n - n_cap) and total/op_cap gates."""
-    from oracle import circuit_lang as cl
+def cpu_baseline_served(args, reqs, budget_s=20.0):
+    """The reference's t_PAR_CPU (FP32, unmodified) on the served stream's requests in order, each run
+    unscaled and alone (one setFunction + execute per request), for about budget_s seconds."""
     from oracle import cpu
 
     threads = os.cpu_count() or 1
-    total_s = 0.0
-    kind = "reference" if cpu.ref_available("f32") else "port"
-    for spec, mask in reqs:
-        full = spec.build(cl.Circuit())
-        t, cm, cv, m = full.as_arrays()
-        n = spec.qubits
-        ns = min(n, n_cap)
-        shift = n - ns
-        keep = [i for i in range(len(t)) if t[i] >= shift and (int(cm[i]) >> shift << shift) == int(cm[i])][:op_cap]
-        ops = (t[keep] - shift, cm[keep] >> shift, cv[keep] >> shift, m[keep])
-        s0 = cpu.basis_state(ns, spec.init_index >> shift, np.complex64)
-        if kind == "reference":
-            dt = ref_replay(ns, s0, ops, threads)
-        else:
-            t0 = time.perf_counter()
-            cpu.run_regions(s0, ns, ops, prec="f32", threads=threads)
-            dt = time.perf_counter() - t0
-        total_s += dt * (1 << shift) * (len(t) / max(1, len(keep)))
-    return {"value": round(len(reqs) / total_s, 6), "unit": "circuits/s", "cores": threads, "kind": kind,
-            "sample": f"{len(reqs)} requests of the served mix on t_PAR_CPU FP32; each run on <= {n_cap} qubits "
-                      f"and its first <= {op_cap} gates, time scaled by state size and gate count"}
+    if not cpu.ref_available("f32"):
+        return None
+    specs = [spec for spec, _ in reqs]
+    done, spent, _, _ = ref_stream(specs, "f32", threads, budget_s)
+    return {"value": round(done / spent, 6), "unit": "circuits/s", "cores": threads, "kind": "reference",
+            "sample": f"the first {done} requests of the timed stream on t_PAR_CPU FP32, each unscaled, one "
+                      f"setFunction + execute per request ({spent:.1f} s)"}
+
 
 WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": workload_grover,
              "batched": workload_batched, "hadamard": workload_hadamard}
+
+METRICS = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
+           "grover": "Grover iterations/s (26q FP64, marked index 42)",
+           "hadamard": "gate-layers/s (H on every qubit, 30q FP64)",
+           "batched": "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
+           "served": SERVED_METRIC}
+
+
+def config_for(args):
+    """The `config` of a workload's JSON line: what the workload is, identical in both arms (engine-side
+    figures such as passes per step go in the line's `plan` key)."""
+    w = args.workload
+    if w == "served":
+        count = args.requests or 48
+        return {"workload": f"served-mix-{count}req", "requests_per_step": count, "rate_hz": args.rate,
+                "max_inflight": args.inflight, "budget_bytes": 150 << 30,
+                "precision": "fp32 amplitudes, fp64 gate matrices, norms and argmax",
+                "mix": "60% layered 12-26q d20, 30% QFT 16-28q, 10% Grover 14-20q",
+                "stream": "step s draws its requests from seed 1000 + s",
+                "l2": "states up to 2 GiB; no flush (serving keeps states resident)"}
+    if w == "batched":
+        count = args.requests or 512
+        return {"workload": f"batched-{count}", "circuits": count, "qubits": "uniform 10-22",
+                "mix": "half QFT of a random basis input, half 10-layer random Rz/Ry+CNOT",
+                "l2": "arena of all states (~2.6 GB FP32) > 126 MB L2, no flush needed"}
+    if w == "layered":
+        n, layers = args.qubits or 30, args.layers or 40
+        S = (1 << n) * (16 if args.precision == "f64" else 8)
+        return {"workload": f"layered-{n}q-{layers}layers", "qubits": n, "layers": layers,
+                "precision": {"f64": "fp64", "f32": "fp32"}[args.precision], "state_bytes": S,
+                "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"}
+    if w == "hadamard":
+        n = args.qubits or 30
+        S = 16 << n
+        return {"workload": f"hadamard-layer-{n}q-fp64", "qubits": n, "gates_per_layer": n, "state_bytes": S,
+                "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"}
+    if w == "grover":
+        n = args.qubits or GROVER_N
+        S = 16 << n
+        return {"workload": f"grover-{n}q-fp64", "qubits": n, "marked": GROVER_MARK,
+                "iterations_per_step": GROVER_STEP_ITERS, "state_bytes": S,
+                "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"}
+    return {"workload": w}
 
 
 def base_line(args, dist, metric, value, unit, ms_step, dtype, config):
@@ -942,28 +963,71 @@ def base_line(args, dist, metric, value, unit, ms_step, dtype, config):
             "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": config}
 
 
+def reference_stream_specs(args):
+    """The circuits of the workload as a stream, in the order the repo arm's timed steps run them."""
+    if args.workload == "served":
+        count = args.requests or 48
+        return [spec for s in range(args.warmup, args.warmup + args.steps + 4)
+                for spec, _ in served_requests(1000 + s, count)], "f32"
+    if args.workload == "batched":
+        return batched_specs(4242, args.requests or 512), "f32"
+    return None, None
+
+
 def reference_arm(args, dist):
-    """The reference's own CPU implementation (t_PAR_CPU), rank 0 only."""
+    """The reference's own CPU implementation (t_PAR_CPU, oracle/_ref), rank 0 only, with every host thread.
+
+    served / batched: each step runs the workload's circuits in stream order, unscaled, one setFunction +
+    execute per circuit as the reference's libraries do, until args.ref_step_s seconds have been spent (the
+    circuit that crosses the budget completes); value = circuits run / seconds.  The other workloads time
+    their bounded, scaled samples (cpu_baseline_*), each a single setFunction + execute."""
     if dist.rank != 0:
         return None
-    fn = {"layered": cpu_baseline_layered,
-          "grover": lambda a: cpu_baseline_grover(a, a.qubits or GROVER_N, GROVER_MARK),
-          "hadamard": lambda a: cpu_baseline_hadamard(a, a.qubits or 30),
-          "batched": lambda a: cpu_baseline_batched(a, batched_specs(4242, a.requests or 512)),
-          "served": lambda a: cpu_baseline_served(a, served_requests(1000 + a.warmup, a.requests or 48))}.get(args.workload)
-    if fn is None:
-        return {"impl": "reference", "unavailable": f"no reference timing for workload {args.workload}"}
-    vals = []
-    for _ in range(max(1, args.steps)):
-        vals.append(fn(args))
-    v = statistics.median([x["value"] for x in vals])
-    first = vals[0]
-    line = {"metric": args.metric_name, "value": v, "unit": first["unit"], "n_gpus": dist.world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "f64",
-            "data": "synthetic (seeded)", "config": {"workload": args.workload},
-            "cpu_baseline": {"value": v, "unit": first["unit"], "cores": first["cores"], "kind": first["kind"],
-                             "sample": first["sample"]},
-            "e2e": {"value": v, "unit": first["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    from oracle import cpu
+
+    threads = os.cpu_count() or 1
+    specs, prec = reference_stream_specs(args)
+    line = {"metric": METRICS.get(args.workload, args.workload), "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "impl": "reference", "data": "synthetic (seeded)", "config": config_for(args)}
+    if specs is not None:
+        if not cpu.ref_available(prec):
+            return {"impl": "reference", "unavailable": "the reference engine (oracle/_ref) was not built"}
+        small = min(specs, key=lambda s: (s.qubits, s.n_ops_estimate()))
+        for _ in range(args.warmup):
+            ref_run_request(small, prec, threads)
+        done, spent, each, cursor = 0, 0.0, [], 0
+        for _ in range(args.steps):
+            d, s, e, cursor = ref_stream(specs, prec, threads, args.ref_step_s, cursor)
+            done, spent, each = done + d, spent + s, each + e
+        v = done / spent
+        unit = "circuits/s"
+        sample = (f"the first {done} circuits of the stream (the timed steps' circuits in order), each unscaled, "
+                  f"one setFunction + execute per circuit on t_PAR_CPU {prec.upper()} "
+                  f"({args.steps} steps of >= {args.ref_step_s:g} s, {spent:.1f} s in all)")
+        line.update({"value": round(v, 6), "unit": unit, "ms_per_step": round(spent / args.steps * 1e3, 3),
+                     "dtype": prec, "circuits_run": done,
+                     "latency_ms": {"p50": round(float(np.percentile(each, 50)) * 1e3, 3),
+                                    "p99": round(float(np.percentile(each, 99)) * 1e3, 3),
+                                    "note": "each circuit's run time alone (sequential, no queueing)"}})
+    else:
+        fn = {"layered": cpu_baseline_layered,
+              "grover": lambda a: cpu_baseline_grover(a, a.qubits or GROVER_N, GROVER_MARK),
+              "hadamard": lambda a: cpu_baseline_hadamard(a, a.qubits or 30)}.get(args.workload)
+        if fn is None:
+            return {"impl": "reference", "unavailable": f"no reference timing for workload {args.workload}"}
+        for _ in range(args.warmup):
+            fn(args)
+        t0 = time.perf_counter()
+        vals = [fn(args) for _ in range(max(1, args.steps))]
+        wall = time.perf_counter() - t0
+        v = statistics.median([x["value"] for x in vals])
+        unit, sample = vals[0]["unit"], vals[0]["sample"]
+        line.update({"value": v, "unit": unit, "ms_per_step": round(wall / max(1, args.steps) * 1e3, 3),
+                     "dtype": "f64"})
+    line["cpu_baseline"] = {"value": line["value"], "unit": unit, "cores": threads, "kind": "reference",
+                            "sample": sample}
+    line["e2e"] = {"value": line["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     return line
 
 
@@ -986,16 +1050,13 @@ def main():
     ap.add_argument("--qubits", type=int, default=0, help="override the workload's qubit count (profiling runs)")
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")
+    ap.add_argument("--ref-step-s", type=float, default=5.0,
+                    help="reference arm, served/batched: seconds of reference work per step")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if args.workload == "served" else 5
     if args.warmup is None:
         args.warmup = 5 if args.workload == "served" else 3
-    args.metric_name = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
-                        "grover": "Grover iterations/s (26q FP64, marked index 42)",
-                        "hadamard": "gate-layers/s (H on every qubit, 30q FP64)",
-                        "batched": "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
-                        "served": SERVED_METRIC}.get(args.workload, args.workload)
     dist = Dist()
     try:
         if args.impl == "reference":

@@ -147,10 +147,23 @@ int hgm_execute(hgm_state *s, const hgm_plan *p, int iterations, void *stream);
 int hgm_norm(hgm_state *s, double *out);
 /* Probability that index bit `bit` is 1 (DGM::measure's sums, dgm_core.cpp:79-84). */
 int hgm_prob_one(hgm_state *s, int bit, double *out);
-/* DGM::measure(qubit) (dgm_core.cpp:69-125) on the device: outcome 0 if
- * P(0) > sample else 1, then collapse and renormalise.  Returns the outcome
- * and the probability of that outcome. */
+/* DGM::measure(qubit) (dgm_core.cpp:69-125) on the device, with the uniform
+ * sample in [0, 1) supplied by the caller: outcome 0 if P(0) > sample else 1.
+ * As in the reference, the measured branch is renormalised and moved to the
+ * qubit's |0> half and the |1> half is cleared, so the qubit is left in |0>
+ * whichever value was read (dgm_core.cpp:115-122).  Returns the outcome and
+ * its probability. */
 int hgm_measure_qubit(hgm_state *s, int qubit, double sample, int *outcome, double *prob);
+/* DGM::colapse(qubit, value) (dgm_core.cpp:129-146): keeps the amplitudes in
+ * which `qubit` has `value`, renormalised, and clears the others; returns the
+ * probability that was collapsed onto (the reference prints it). */
+int hgm_collapse_qubit(hgm_state *s, int qubit, int value, double *prob);
+/* DGM::measure(vector<int>) (dgm_core.cpp:150-162): the probabilities of every
+ * value of the index bits in `mask`, summed over the other bits, without
+ * collapsing; out[x] for x = 0 .. 2^popcount(mask)-1, where bit j of x is the
+ * j-th lowest bit of `mask` (the reference keys the same sums by
+ * index & mask).  count must be 2^popcount(mask), at most 2^26. */
+int hgm_marginal_probs(hgm_state *s, uint64_t mask, double *out, int64_t count);
 /* Marginal distribution over the index bits in `mask`: argmax of
  * sum over the other bits of |a|^2 (ties -> lowest index). */
 int hgm_marginal_argmax(hgm_state *s, uint64_t mask, int64_t *arg, double *prob);
@@ -162,17 +175,22 @@ int hgm_max_abs_diff(hgm_state *a, hgm_state *b, double *out);
 int hgm_scale(hgm_state *s, double scale);
 
 /* Allocation-free FP64 norm: sum |a|^2 of the device state `d_state`
- * (2^qubits amplitudes of the given precision), written to the device
- * double `d_out`, queued on `stream` (NULL: the legacy default stream).
- * No counterpart in the reference.  For callers that cannot allocate device
- * memory (code inside a framework that owns every allocation, or running
- * while another thread captures a CUDA graph): it calls no cudaMalloc,
- * cudaFree or allocating routine and keeps its partial sums in an 18.5 KiB
- * device array that every GPU loading this library holds until exit.
- * Limit: 1..34 qubits (HGM_ERR_UNSUPPORTED beyond).  All calls share that
- * array: calls that overlap on the GPU race and must be serialised.  The
- * first call on a device looks the array's address up (make it before any
- * stream capture). */
+ * (2^qubits amplitudes of the given precision), written to the one device
+ * double at `d_out` (8 bytes; nothing after it is touched), queued on
+ * `stream`.  No counterpart in the reference.  For callers that cannot
+ * allocate device memory (code inside a framework that owns every
+ * allocation and hands this library only its buffers, or code running while
+ * another thread captures a CUDA graph, where an allocation would break the
+ * capture): it calls no cudaMalloc, cudaFree or allocating routine and keeps
+ * its partial sums in an 18.5 KiB device array that every GPU loading this
+ * library holds until exit.  Limit: 1..34 qubits, the engine's state range
+ * (HGM_ERR_UNSUPPORTED beyond; the array itself fits any size, the grid
+ * being capped at its 1184 partials).  All calls share that array: calls
+ * that overlap on the GPU race and must be serialised.  The first call on a
+ * device looks the array's address up (make it before any stream capture).
+ * stream NULL is the legacy default stream, which synchronises with every
+ * blocking stream: while another thread captures on a blocking stream, pass
+ * a stream created with cudaStreamNonBlocking instead. */
 int hgm_norm_noalloc(const void *d_state, int qubits, int precision, double *d_out, void *stream);
 
 /* ---- batched mode --------------------------------------------------------- */
@@ -205,6 +223,13 @@ int hgm_batch_set_inputs(hgm_batch *b, const int64_t *init_index, void *stream);
 int hgm_batch_download(hgm_batch *b, void *host, int64_t bytes, void *stream);
 /* After a run has completed: HGM_ERR_TIMEOUT if a tile gave up waiting. */
 int hgm_batch_check(hgm_batch *b);
+/* Fault injection for tests, made on the host: from the next run, `task`
+ * (an index into the finalized batch's task table; it must have a
+ * dependency) waits for one completion more than its dependency can give,
+ * and every dependency wait gives up after wait_ns instead of 2 s, so the
+ * run ends with HGM_ERR_TIMEOUT from hgm_batch_check.  task < 0 restores the
+ * normal table and limit.  Waits for earlier runs first. */
+int hgm_batch_inject_stall(hgm_batch *b, int task, int64_t wait_ns);
 /* pass_bytes: the algorithmic bytes of one run, a read and a write of a
  * state per pass (per task). */
 int hgm_batch_size(const hgm_batch *b, int *jobs, int64_t *tasks, int64_t *items, int64_t *arena_bytes,

@@ -9,5 +9,7 @@ leg import this package, and only to check results against.  The product package
                  and, when it was built here, to the reference's own engine
                  (oracle/_ref/libref_{f32,f64}.so).
 * closed_forms   analytic states: H benchmark, Grover, QFT of a basis state.
-* workloads      seeded synthetic circuits of the benchmark shapes.
+
+The seeded benchmark circuits themselves are built by the product package's
+simulador_quantico_b200/workloads.py (circuit strings only, no engine code).
 """

@@ -21,8 +21,8 @@
 #                               libhgm_dropin_{f32,f64}.so (only when those
 #                               exist)
 #
-# Sources are read where they lie under the reference tree (REF_ROOT,
-# default /root/reference); the widened copy is written to a scratch folder
+# Sources are read where they lie under the reference tree, whose root the
+# caller names in REF_ROOT (required; nothing is built without it); the widened copy is written to a scratch folder
 # under oracle/_ref/ and removed after compilation.  Compiler flags follow
 # the reference makefile (makefile:33,92): -O3 -fopenmp -fcx-limited-range
 # on the four engine files, default flags elsewhere; -fPIC is added so the
@@ -31,10 +31,14 @@ set -euo pipefail
 
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REPO="$(cd "$HERE/.." && pwd)"
-REF_ROOT="${REF_ROOT:-/root/reference}"
+REF_ROOT="${REF_ROOT:-}"
 OUT="$HERE/_ref"
 DROPIN_DIR="$REPO/simulador_quantico_b200/lib"
 
+if [ -z "$REF_ROOT" ]; then
+    echo "build_ref.sh: REF_ROOT (the reference tree's root) is not set; keeping existing oracle/_ref" >&2
+    exit 0
+fi
 if [ ! -d "$REF_ROOT/src/core" ]; then
     echo "build_ref.sh: reference tree not found at $REF_ROOT; keeping existing oracle/_ref" >&2
     exit 0

@@ -158,6 +158,12 @@ class RefDGM:
             L.ref_dgm_measure.argtypes = [C.c_void_p, C.c_int]
             L.ref_dgm_measure.restype = C.c_int
             L.ref_seed_rng.argtypes = [C.c_ulong]
+            L.ref_uniform_sample.argtypes = [C.c_ulong]
+            L.ref_uniform_sample.restype = C.c_double
+            L.ref_dgm_colapse.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            L.ref_dgm_measure_many.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_long),
+                                               C.POINTER(C.c_double), C.c_long]
+            L.ref_dgm_measure_many.restype = C.c_long
             cls._libs[key] = L
         return cls._libs[key]
 
@@ -222,3 +228,19 @@ class RefDGM:
 
     def seed(self, s):
         self.lib.ref_seed_rng(s)
+
+    def uniform_sample(self, s):
+        """The sample measure() draws first after seed(s); leaves the generator seeded with s."""
+        return self.lib.ref_uniform_sample(s)
+
+    def colapse(self, qubit, value):
+        self.lib.ref_dgm_colapse(self.h, qubit, value)
+
+    def measure_many(self, qubits):
+        """DGM::measure(vector<int>): {index & mask: probability}."""
+        q = (C.c_int * len(qubits))(*qubits)
+        cap = 1 << len(qubits)
+        keys = (C.c_long * cap)()
+        probs = (C.c_double * cap)()
+        n = self.lib.ref_dgm_measure_many(self.h, q, len(qubits), keys, probs, cap)
+        return {int(keys[k]): float(probs[k]) for k in range(min(n, cap))}

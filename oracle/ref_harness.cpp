@@ -19,6 +19,8 @@
 #include "core/gates.h"
 #include <cstring>
 #include <cstdint>
+#include <random>
+#include <vector>
 
 #ifndef REF_REAL
 #error "REF_REAL must be defined (float or double)"
@@ -140,5 +142,36 @@ void ref_dgm_execute(void *h, int iterations) {
 void ref_seed_rng(unsigned long seed) { seed_rng(seed); }
 
 int ref_dgm_measure(void *h, int qubit) { return ((DGM *)h)->measure(qubit); }
+
+// The uniform sample DGM::measure(int) draws first after seed_rng(seed)
+// (src/core/dgm_core.cpp:97-101: a uniform_real_distribution<double>(0, 1) on
+// g_rng); g_rng is re-seeded with `seed` afterwards, so the next measure draws
+// the same value.
+double ref_uniform_sample(unsigned long seed) {
+    seed_rng(seed);
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    const double v = dist(g_rng);
+    seed_rng(seed);
+    return v;
+}
+
+// DGM::colapse(qubit, value) (src/core/dgm_core.cpp:129-146).
+void ref_dgm_colapse(void *h, int qubit, int value) { ((DGM *)h)->colapse(qubit, value); }
+
+// DGM::measure(vector<int>) (src/core/dgm_core.cpp:150-162): its map's keys
+// (index & mask) and probabilities, in key order; returns the map's size.
+long ref_dgm_measure_many(void *h, const int *qubits, int nq, long *keys, double *probs, long cap) {
+    std::vector<int> pos(qubits, qubits + nq);
+    auto m = ((DGM *)h)->measure(pos);
+    long k = 0;
+    for (auto &kv : m) {
+        if (k < cap) {
+            keys[k] = kv.first;
+            probs[k] = (double)kv.second;
+        }
+        k++;
+    }
+    return k;
+}
 
 }  // extern "C"

@@ -81,6 +81,8 @@ def _load():
         "hgm_norm": ([vp, P(d)], i),
         "hgm_prob_one": ([vp, i, P(d)], i),
         "hgm_measure_qubit": ([vp, i, d, P(i), P(d)], i),
+        "hgm_collapse_qubit": ([vp, i, i, P(d)], i),
+        "hgm_marginal_probs": ([vp, C.c_uint64, P(d), i64], i),
         "hgm_marginal_argmax": ([vp, C.c_uint64, P(i64), P(d)], i),
         "hgm_inner": ([vp, vp, P(d), P(d)], i),
         "hgm_max_abs_diff": ([vp, vp, P(d)], i),
@@ -97,6 +99,7 @@ def _load():
         "hgm_pinned_alloc": ([i64, P(vp)], i),
         "hgm_pinned_free": ([vp], None),
         "hgm_batch_check": ([vp], i),
+        "hgm_batch_inject_stall": ([vp, i, i64], i),
         "hgm_batch_size": ([vp, P(i), P(i64), P(i64), P(i64), P(i64)], i),
         "hgm_batch_state": ([vp, i], vp),
         "hgm_server_default_opts": ([P(ServerOpts), i], None),

@@ -9,8 +9,9 @@
 // pass 1, ...), and the CTAs of one persistent grid claim tiles in that
 // order from a global counter.  A tile of pass p may start only when every
 // tile of pass p-1 of the same circuit is done: the claiming thread spins on
-// that task's completion counter with a time limit (2 s of %globaltimer),
-// after which it sets an error flag and the CTA skips the tile.  Because a
+// that task's completion counter with a time limit (2 s of %globaltimer by
+// default; the limit is a field of the task), after which it sets an error
+// flag and the CTA skips the tile.  Because a
 // tile only ever waits for tiles claimed before it, and a claimed tile is
 // already held by a running CTA, the queue always makes progress, whether
 // or not all CTAs are resident.
@@ -31,6 +32,8 @@ struct BatchTask {
     long long tile_begin;   // first global item of this task
     int32_t ntiles;
     int32_t dep;            // task that must be complete first, -1 if none
+    uint32_t dep_need;      // completions of `dep` to wait for (its tile count)
+    unsigned long long wait_ns;  // limit of that wait
     int32_t small;          // 1: whole circuit in shared memory
     int32_t n;              // qubits
     const void *small_ops;  // SmallOp<Real>[] for small tasks
@@ -108,10 +111,11 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
                 s_task = lo;
                 const int dep = tasks[lo].dep;
                 if (dep >= 0) {
-                    const unsigned int need = (unsigned int)tasks[dep].ntiles;
+                    const unsigned int need = tasks[lo].dep_need;
+                    const unsigned long long limit = tasks[lo].wait_ns;
                     const unsigned long long t0 = global_ns();
                     while (ld_acquire(&done[dep]) < need) {
-                        if (global_ns() - t0 > BATCH_WAIT_LIMIT_NS) {
+                        if (global_ns() - t0 > limit) {
                             atomicExch(error, 1);
                             s_skip = 1;
                             break;
@@ -302,6 +306,8 @@ int batch_finalize(Batch *b) {
                 t.pa.flags = 0;
                 t.ntiles = 1 << (j.n - t.pa.k);
             }
+            t.dep_need = t.dep >= 0 ? (uint32_t)b->tasks[t.dep].ntiles : 0u;
+            t.wait_ns = BATCH_WAIT_LIMIT_NS;
             t.tile_begin = b->total_items;
             b->total_items += t.ntiles;
             task_of[ji].push_back((int)b->tasks.size());
@@ -495,6 +501,25 @@ int hgm_batch_check(hgm_batch *bb) {
     cudaError_t e = cudaMemcpy(&err, b->d_error, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_err(e, "batch error flag");
     return err ? fail(HGM_ERR_TIMEOUT, "a batched tile gave up waiting for its previous pass") : HGM_OK;
+}
+
+int hgm_batch_inject_stall(hgm_batch *bb, int task, int64_t wait_ns) {
+    Batch *b = reinterpret_cast<Batch *>(bb);
+    if (!b || !b->finalized) return fail(HGM_ERR_INVALID, "batch not finalized");
+    if (task >= (int)b->tasks.size()) return fail(HGM_ERR_INVALID, "no task %d", task);
+    if (task >= 0 && b->tasks[task].dep < 0) return fail(HGM_ERR_INVALID, "task %d has no dependency", task);
+    if (task >= 0 && wait_ns <= 0) return fail(HGM_ERR_INVALID, "wait limit must be positive");
+    for (size_t k = 0; k < b->tasks.size(); k++) {
+        BatchTask &t = b->tasks[k];
+        t.dep_need = t.dep >= 0 ? (uint32_t)b->tasks[t.dep].ntiles : 0u;
+        t.wait_ns = task >= 0 ? (unsigned long long)wait_ns : BATCH_WAIT_LIMIT_NS;
+    }
+    if (task >= 0) b->tasks[task].dep_need += 1;  // one completion more than the dependency has tiles
+    // earlier replays read the table: let them finish before it changes
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_tasks, b->tasks.data(), b->tasks.size() * sizeof(BatchTask), cudaMemcpyHostToDevice);
+    return cuda_err(e, "batch task table");
 }
 
 int hgm_batch_size(const hgm_batch *bb, int *jobs, int64_t *tasks, int64_t *items, int64_t *arena_bytes,

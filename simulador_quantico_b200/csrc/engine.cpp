@@ -242,11 +242,42 @@ int hgm_measure_qubit(hgm_state *s, int qubit, double sample, int *outcome, doub
     const int value = (zero > sample) ? 0 : 1;
     const double p = value ? one : zero;
     if (!(p > 0)) return fail(HGM_ERR_INVALID, "measured outcome has zero probability");
-    rc = collapse(st, bit, value, 1.0 / std::sqrt(p), nullptr);
+    // the measured branch, rescaled, moves to the qubit's |0> half
+    // (dgm_core.cpp:117-122)
+    rc = measure_update(st, bit, value, 1.0 / std::sqrt(p), nullptr);
     if (rc) return rc;
     if (outcome) *outcome = value;
     if (prob) *prob = p;
     return HGM_OK;
+}
+
+int hgm_collapse_qubit(hgm_state *s, int qubit, int value, double *prob) {
+    State *st = reinterpret_cast<State *>(s);
+    if (!st) return fail(HGM_ERR_INVALID, "null state");
+    if (qubit < 0 || qubit >= st->qubits) return fail(HGM_ERR_INVALID, "qubit %d outside state", qubit);
+    if (value != 0 && value != 1) return fail(HGM_ERR_INVALID, "value %d is not 0 or 1", value);
+    const int bit = st->qubits - 1 - qubit;
+    double total = 0, one = 0;
+    int rc = reduce_norm(st, &total, nullptr);
+    if (!rc) rc = reduce_prob_one(st, bit, &one, nullptr);
+    if (rc) return rc;
+    const double p = value ? one : total - one;
+    if (!(p > 0)) return fail(HGM_ERR_INVALID, "collapse onto a value of zero probability");
+    // DGM::colapse (dgm_core.cpp:129-146): keep the amplitudes whose qubit has
+    // `value`, divide them by sqrt of their probability, clear the rest
+    rc = collapse(st, bit, value, 1.0 / std::sqrt(p), nullptr);
+    if (rc) return rc;
+    if (prob) *prob = p;
+    return HGM_OK;
+}
+
+int hgm_marginal_probs(hgm_state *s, uint64_t mask, double *out, int64_t count) {
+    State *st = reinterpret_cast<State *>(s);
+    if (!st || !out) return fail(HGM_ERR_INVALID, "null argument");
+    const int m = __builtin_popcountll(mask);
+    if (m > 62 || count != (int64_t(1) << m))
+        return fail(HGM_ERR_INVALID, "output holds %lld values, the mask needs 2^%d", (long long)count, m);
+    return marginal_probs(st, mask, out, nullptr);
 }
 
 int hgm_marginal_argmax(hgm_state *s, uint64_t mask, int64_t *arg, double *prob) {

@@ -243,7 +243,9 @@ int launch_set_basis(State *s, int64_t index, void *stream);
 int reduce_norm(State *s, double *out, void *stream);
 int reduce_prob_one(State *s, int bit, double *out, void *stream);
 int collapse(State *s, int bit, int value, double inv_norm, void *stream);
+int measure_update(State *s, int bit, int value, double inv_norm, void *stream);
 int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *stream);
+int marginal_probs(State *s, uint64_t mask, double *host_out, void *stream);
 int inner(State *a, State *b, double *re, double *im, void *stream);
 int max_abs_diff(State *a, State *b, double *out, void *stream);
 int scale_state(State *s, double scale, void *stream);

@@ -326,6 +326,26 @@ __global__ void collapse_kernel(typename V2<Real>::T *s, long long N, int bit, i
     }
 }
 
+// DGM::measure(int)'s state update (src/core/dgm_core.cpp:117-122): for every
+// pair of indices differing only in `bit`, the amplitude of the measured
+// branch, rescaled, goes to the bit-0 index and the bit-1 index is cleared,
+// so the measured qubit is left in |0> whichever value was read.  One thread
+// per pair: the pair's two amplitudes are read before either is written.
+template <typename Real>
+__global__ void measure_update_kernel(typename V2<Real>::T *s, long long half, int bit, int value, double inv_norm) {
+    const long long low = (1ll << bit) - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < half; p += (long long)gridDim.x * blockDim.x) {
+        const long long i0 = ((p & ~low) << 1) | (p & low), i1 = i0 | (1ll << bit);
+        typename V2<Real>::T v = s[value ? i1 : i0], z;
+        v.x = (Real)(v.x * inv_norm);
+        v.y = (Real)(v.y * inv_norm);
+        z.x = 0;
+        z.y = 0;
+        s[i0] = v;
+        s[i1] = z;
+    }
+}
+
 template <typename Real>
 __global__ void scale_kernel(typename V2<Real>::T *s, long long N, double f) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
@@ -359,6 +379,17 @@ int collapse(State *s, int bit, int value, double inv_norm, void *stream) {
     else collapse_kernel<float><<<grid_for(N), 256, 0, st>>>((float2 *)s->d, N, bit, value, inv_norm);
     count_launch();
     return check("collapse");
+}
+
+int measure_update(State *s, int bit, int value, double inv_norm, void *stream) {
+    cudaStream_t st = pick(stream);
+    const long long half = 1ll << (s->qubits - 1);
+    if (s->precision == HGM_F64)
+        measure_update_kernel<double><<<grid_for(half), 256, 0, st>>>((double2 *)s->d, half, bit, value, inv_norm);
+    else
+        measure_update_kernel<float><<<grid_for(half), 256, 0, st>>>((float2 *)s->d, half, bit, value, inv_norm);
+    count_launch();
+    return check("measure update");
 }
 
 int scale_state(State *s, double f, void *stream) {
@@ -671,6 +702,85 @@ static int queue_marginal(State *s, uint64_t mask, double *pbest, long long *ibe
     return check("argmax launch");
 }
 
+// The whole marginal distribution over the bits of `mask` (DGM::measure(vector),
+// src/core/dgm_core.cpp:150-162): out[x] = sum over the other bits of |a|^2,
+// for every value x of the mask bits (bit j of x is the j-th lowest mask bit).
+__global__ void marginal_chunks_sum(const double *partial, long long M, int nch, double *out) {
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < M; x += (long long)gridDim.x * blockDim.x) {
+        double p = 0.0;
+        for (int k = 0; k < nch; k++) p += partial[x * nch + k];
+        out[x] = p;
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(RED_THREADS) marginal_values_kernel(const typename V2<Real>::T *__restrict__ s, int n,
+                                                                       unsigned long long mask, int m, double *out) {
+    const unsigned long long comp = ~mask & ((n >= 64) ? ~0ull : ((1ull << n) - 1));
+    const long long M = 1ll << m, C = 1ll << (n - m);
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < M; x += (long long)gridDim.x * blockDim.x) {
+        unsigned long long base = 0, src = (unsigned long long)x, mm = mask;
+        while (mm) {
+            const int g = __ffsll((long long)mm) - 1;
+            mm &= mm - 1;
+            base |= (src & 1ull) << g;
+            src >>= 1;
+        }
+        double p = 0.0;
+        for (long long c = 0; c < C; c++) {
+            unsigned long long idx = base, cs = (unsigned long long)c, cm = comp;
+            while (cm) {
+                const int g = __ffsll((long long)cm) - 1;
+                cm &= cm - 1;
+                idx |= (cs & 1ull) << g;
+                cs >>= 1;
+            }
+            const typename V2<Real>::T v = s[idx];
+            p += (double)v.x * v.x + (double)v.y * v.y;
+        }
+        out[x] = p;
+    }
+}
+
+int marginal_probs(State *s, uint64_t mask, double *host_out, void *stream) {
+    if (ensure_ctx()) return HGM_ERR_CUDA;
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    const int n = s->qubits;
+    if (n < 64 && (mask >> n)) return fail(HGM_ERR_INVALID, "mask beyond state bits");
+    const int m = __builtin_popcountll(mask);
+    if (m > 26) return fail(HGM_ERR_UNSUPPORTED, "marginal over %d bits (at most 26)", m);
+    const long long M = 1ll << m;
+    double *d_out = nullptr;
+    cudaError_t e = cudaMallocAsync(&d_out, (size_t)M * sizeof(double), st);
+    if (e != cudaSuccess) return fail(HGM_ERR_NOMEM, "marginal output: %s", cudaGetErrorString(e));
+    if (M <= RED_BLOCKS) {
+        const int nch = (int)(RED_BLOCKS / M);
+        const unsigned g = (unsigned)(M * nch);
+        if (s->precision == HGM_F64)
+            marginal_chunk_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, nch, g_ctx.partials);
+        else
+            marginal_chunk_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, nch, g_ctx.partials);
+        marginal_chunks_sum<<<(unsigned)((M + 255) / 256), 256, 0, st>>>(g_ctx.partials, M, nch, d_out);
+    } else {
+        unsigned g = (unsigned)((M + RED_THREADS - 1) / RED_THREADS);
+        if (g > RED_BLOCKS) g = RED_BLOCKS;
+        if (s->precision == HGM_F64)
+            marginal_values_kernel<double><<<g, RED_THREADS, 0, st>>>((const double2 *)s->d, n, mask, m, d_out);
+        else
+            marginal_values_kernel<float><<<g, RED_THREADS, 0, st>>>((const float2 *)s->d, n, mask, m, d_out);
+    }
+    count_launch(2);
+    int rc = check("marginal probabilities launch");
+    if (!rc) {
+        e = cudaMemcpyAsync(host_out, d_out, (size_t)M * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = fail(HGM_ERR_CUDA, "marginal probabilities: %s", cudaGetErrorString(e));
+    }
+    cudaFreeAsync(d_out, st);
+    return rc;
+}
+
 int launch_argmax_async(State *s, uint64_t mask, double *pbest, long long *ibest, double *out, void *stream) {
     return queue_marginal(s, mask, pbest, ibest, out, (cudaStream_t)stream);
 }
@@ -696,6 +806,9 @@ int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *s
 // framework that owns every device allocation (a plugin handed pre-allocated
 // buffers), or code running while a CUDA graph is being captured elsewhere
 // in the process, where a cudaMalloc would be illegal or would synchronise.
+// Such a caller should queue it on a stream created non-blocking: the legacy
+// default stream (stream NULL) synchronises with blocking streams, and a
+// launch there while one of them captures invalidates that capture.
 // This variant of the FP64 norm reduction keeps its per-block partial sums in
 // a file-scope device array, so it allocates nothing: the caller passes the
 // state and a device location for the result.
@@ -703,8 +816,12 @@ int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *s
 // Limits and sharing:
 //   * the array holds NOALLOC_PARTIALS = 2*1184 doubles (18.5 KiB) on every
 //     GPU that loads this library, for the life of the process;
-//   * a reduction uses at most 1184 blocks (one partial each), so any state
-//     of 1..34 qubits fits; more qubits are rejected with HGM_ERR_UNSUPPORTED;
+//   * the reduction grid is capped at 1184 blocks (one partial each) for any
+//     state size, so the array never limits the size; the qubit range
+//     1..34 is the engine's own state range (hgm_state_create), and more
+//     qubits are rejected with HGM_ERR_UNSUPPORTED;
+//   * the result is exactly one double at d_out: the final step writes
+//     d_out[0] and nothing after it;
 //   * every call shares the array; each call writes every partial it reads
 //     before reading it, so nothing needs clearing, but calls that overlap
 //     on the GPU (different streams, or different host threads) race on it
@@ -714,6 +831,16 @@ int marginal_argmax(State *s, uint64_t mask, int64_t *arg, double *prob, void *s
 //     call before any stream capture.
 constexpr int NOALLOC_PARTIALS = 2 * RED_BLOCKS;
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_PARTIALS];
+
+// Final step of the allocation-free norm: sums the block partials in the same
+// fixed order as reduce_final and writes the one result double.
+__global__ void noalloc_norm_final(const double *partials, int nblocks, double *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double t0 = 0.0;
+        for (int k = 0; k < nblocks; k++) t0 += partials[2 * k];
+        out[0] = t0;
+    }
+}
 
 namespace {
 std::mutex g_noalloc_mu;
@@ -744,8 +871,7 @@ extern "C" int hgm_norm_noalloc(const void *d_state, int qubits, int precision, 
     if (!d_state || !d_out) return fail(HGM_ERR_INVALID, "null state or output pointer");
     if (precision != HGM_F64 && precision != HGM_F32) return fail(HGM_ERR_INVALID, "bad precision");
     if (qubits < 1 || qubits > 34)
-        return fail(HGM_ERR_UNSUPPORTED, "qubits=%d outside 1..34 (the scratch holds %d block partials)", qubits,
-                    NOALLOC_PARTIALS / 2);
+        return fail(HGM_ERR_UNSUPPORTED, "qubits=%d outside 1..34, the engine's state range", qubits);
     double *partials = nullptr;
     int rc = noalloc_scratch(&partials);
     if (rc) return rc;
@@ -758,7 +884,7 @@ extern "C" int hgm_norm_noalloc(const void *d_state, int qubits, int precision, 
     else
         reduce_kernel<float, float, RED_NORM><<<g, RED_THREADS, 0, st>>>((const float2 *)d_state, nullptr, N, 0,
                                                                           partials);
-    reduce_final<RED_NORM><<<1, 32, 0, st>>>(partials, (int)g, d_out);
+    noalloc_norm_final<<<1, 32, 0, st>>>(partials, (int)g, d_out);
     count_launch(2);
     return check("hgm_norm_noalloc launch");
 }

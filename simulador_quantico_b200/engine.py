@@ -201,6 +201,17 @@ class State:
         check(lib.hgm_measure_qubit(self.h, qubit, sample, C.byref(o), C.byref(p)))
         return o.value, p.value
 
+    def collapse_qubit(self, qubit: int, value: int) -> float:
+        p = C.c_double()
+        check(lib.hgm_collapse_qubit(self.h, qubit, value, C.byref(p)))
+        return p.value
+
+    def marginal_probs(self, mask: int):
+        """Probabilities of every value of the mask bits (bit j of the index = j-th lowest mask bit)."""
+        out = np.empty(1 << bin(mask).count("1"), dtype=np.float64)
+        check(lib.hgm_marginal_probs(self.h, mask, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        return out
+
     def marginal_argmax(self, mask: int):
         a, p = C.c_int64(), C.c_double()
         check(lib.hgm_marginal_argmax(self.h, mask, C.byref(a), C.byref(p)))
@@ -269,6 +280,12 @@ class Batch:
 
     def check(self):
         check(lib.hgm_batch_check(self.h))
+
+    def inject_stall(self, task: int, wait_ns: int = 0):
+        """Test hook: task `task` waits on a completion that never comes, every wait limited to wait_ns;
+        task < 0 restores the normal table (hgm_batch_inject_stall)."""
+        check(lib.hgm_batch_inject_stall(self.h, task, wait_ns))
+        return self
 
     def size(self) -> dict:
         j, t, it, ab, pb = C.c_int(), C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
@@ -441,6 +458,25 @@ class DGM:
         """DGM::measure(int) with the uniform sample supplied by the caller."""
         outcome, _ = self.state.measure_qubit(qubit_pos, sample)
         return outcome
+
+    def colapse(self, qubit_pos: int, value: int) -> float:
+        """DGM::colapse (src/core/dgm_core.cpp:129-146); returns the probability collapsed onto."""
+        return self.state.collapse_qubit(qubit_pos, value)
+
+    def measure_positions(self, qubit_positions) -> dict:
+        """DGM::measure(vector<int>) (src/core/dgm_core.cpp:150-162): {index & mask: probability}."""
+        bits = sorted(self.qubits - 1 - q for q in qubit_positions)
+        mask = 0
+        for b in bits:
+            mask |= 1 << b
+        probs = self.state.marginal_probs(mask)
+        out = {}
+        for x, p in enumerate(probs):
+            key = 0
+            for j, b in enumerate(bits):
+                key |= ((x >> j) & 1) << b
+            out[key] = float(p)
+        return out
 
     def host_state(self):
         return self.state.download()

@@ -108,3 +108,37 @@ def test_batch_set_inputs(sq):
     bad[3] = 1 << ns[3]
     with pytest.raises(sq.HgmError):
         b.set_inputs(bad)
+
+
+def test_batch_bounded_wait_times_out(sq):
+    """The persistent kernel's dependency wait is bounded: a task made to wait
+    for a completion that never comes (injected on the host, with a 1 ms
+    limit) gives up, the run ends and hgm_batch_check reports
+    HGM_ERR_TIMEOUT; with the normal table restored the next run is clean and
+    its results match the oracle again."""
+    specs = [wl.random_layered(16, 6, seed=61), wl.random_layered(15, 6, seed=62)]
+    b = sq.Batch("f64", 1)
+    for spec in specs:
+        b.add(spec.build(sq.Circuit()), spec.qubits, spec.init_index)
+    b.finalize()
+    ntasks = b.size()["tasks"]
+    stalled = None
+    for t in range(len(specs), ntasks):  # wave 0 has no dependencies
+        try:
+            b.inject_stall(t, 1_000_000)
+            stalled = t
+            break
+        except sq.HgmError:
+            continue
+    assert stalled is not None
+    b.run()
+    sq.synchronize()
+    with pytest.raises(sq.HgmError) as e:
+        b.check()
+    assert e.value.code == 5  # HGM_ERR_TIMEOUT
+    b.inject_stall(-1)
+    b.run()
+    sq.synchronize()
+    b.check()
+    for j, spec in enumerate(specs):
+        assert np.abs(b.state(j).download() - oracle_state(spec, "f64")).max() < TOL_F64

@@ -1,0 +1,150 @@
+"""Parity at the benchmark sizes: the workloads the benchmark times, checked
+against the oracle or its closed forms at their full sizes.
+
+* Grover search, 26 qubits FP64, marked index 42, all 6433 iterations (the
+  search space and iteration count of grover.out's 27-qubit run,
+  src/algorithms/lib_grover.cpp:53, without the ancilla): the argmax must be
+  42 exactly and every amplitude must match the closed form
+  (oracle/closed_forms.grover_search) within 1e-12.
+* Random layered circuits (Rz/Ry on every qubit, then CNOT on a random
+  matching) at 28 qubits (2 layers) and 30 qubits (1 layer) in FP64, against
+  the oracle's restatement of the reference's t_PAR_CPU engine
+  (oracle/sv_oracle.c, pinned bit for bit to the reference by
+  tests/test_oracle.py) within 1e-12.
+* Textbook QFTs of the serving mix's largest size, 28 qubits: FP64 on the
+  engine within 1e-12 of the closed form (oracle/closed_forms.qft_basis), and
+  FP32 through the serving mode within 1-F < 1e-6 and an amplitude error
+  under 1e-4 of the amplitude's size.
+The host comparisons run in chunks so that a 16 GiB state needs no
+temporaries of its own size.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import circuit_lang as cl
+from oracle import closed_forms as cf
+from oracle import cpu
+from simulador_quantico_b200 import workloads as wl
+from tests.helpers import TOL_F64
+
+pytestmark = pytest.mark.gpu
+
+CHUNK = 1 << 24
+
+
+def host_ram_available():
+    try:
+        import psutil
+
+        return psutil.virtual_memory().available
+    except Exception:
+        return 0
+
+
+def chunked_max_diff(got, want_fn, n):
+    worst = 0.0
+    for lo in range(0, 1 << n, CHUNK):
+        hi = min(lo + CHUNK, 1 << n)
+        w = want_fn(lo, hi)
+        worst = max(worst, float(np.abs(got[lo:hi].astype(np.complex128) - w).max()))
+    return worst
+
+
+def qft_chunk(n, x, lo, hi):
+    N = 1 << n
+    prod = (np.arange(lo, hi, dtype=np.int64) * (x % N)) % N
+    return np.exp(2j * math.pi * prod.astype(np.float64) / N) / math.sqrt(N)
+
+
+def test_grover_search_26q_full(sq):
+    n, mark = 26, 42
+    spec = wl.grover_search(n, mark)
+    k = spec.meta["iterations"]
+    assert k == 6433
+    (h_steps, _, _), (it_steps, _, _) = spec.calls
+    init, one = sq.Circuit(), sq.Circuit()
+    for c in (init, one):
+        for name, m in spec.gates.items():
+            c.add_gate(name, np.asarray(m, dtype=np.complex128))
+    init.set_function(h_steps, 1, True)
+    one.set_function(it_steps, 1, False)
+    st = sq.State(n, "f64").set_basis(0)
+    st.execute(sq.Plan(init, n, "f64")).execute(sq.Plan(one, n, "f64"), k)
+    arg, p = st.marginal_argmax((1 << n) - 1)
+    assert arg == mark
+    got = st.download()
+    st.free()
+    marked, other = cf.grover_amplitudes(n, k)
+    assert abs(got[mark] - marked) < TOL_F64
+    assert abs(p - marked * marked) < 1e-12
+    got[mark] = other
+    assert np.abs(got - other).max() < TOL_F64
+
+
+def layered_case(sq, n, layers, seed):
+    spec = wl.random_layered(n, layers, seed=seed)
+    st = sq.State(n, "f64").set_basis(0)
+    st.execute(sq.Plan(spec.build(sq.Circuit()), n, "f64"))
+    got = st.download()
+    st.free()
+    ops = spec.build(cl.Circuit()).as_arrays()
+    want = cpu.run_regions(cpu.basis_state(n, 0), n, ops, prec="f64")
+    err = chunked_max_diff(got, lambda lo, hi: want[lo:hi], n)
+    scale = float(np.abs(want[: 1 << 20]).max())
+    del want
+    return err, scale
+
+
+def test_layered_28q_f64_vs_oracle(sq):
+    if host_ram_available() < (24 << 30):
+        pytest.skip("needs 24 GiB of host memory")
+    err, scale = layered_case(sq, 28, 2, seed=2801)
+    assert err < TOL_F64
+    assert err < 1e-9 * scale
+
+
+def test_layered_30q_f64_vs_oracle(sq):
+    if host_ram_available() < (80 << 30):
+        pytest.skip("needs 80 GiB of host memory")
+    err, scale = layered_case(sq, 30, 1, seed=3001)
+    assert err < TOL_F64
+    assert err < 1e-9 * scale
+
+
+def test_qft_28q_f64_closed_form(sq):
+    n, x = 28, 0x9E3779B & ((1 << 28) - 1)
+    spec = wl.qft(n, x)
+    st = sq.State(n, "f64").set_basis(x)
+    st.execute(sq.Plan(spec.build(sq.Circuit()), n, "f64"))
+    got = st.download()
+    st.free()
+    assert chunked_max_diff(got, lambda lo, hi: qft_chunk(n, x, lo, hi), n) < TOL_F64
+
+
+def test_qft_28q_f32_served_closed_form(sq):
+    """The serving mix's largest QFT through the FP32 server (keep_states)."""
+    n, x = 28, 0x5A5A5A5 & ((1 << 28) - 1)
+    spec = wl.qft(n, x)
+    srv = sq.Server("f32", budget_bytes=8 << 30, max_inflight=2, keep_states=True)
+    rid = srv.submit(spec.build(sq.Circuit()), n, x, 0)
+    (res,) = srv.drain(1)
+    assert res["status"] == 0 and res["id"] == rid
+    got = srv.result_state(rid).download()
+    srv.release(rid)
+    srv.close()
+    amp = 2.0 ** (-n / 2)
+    ov, nrm = 0j, 0.0
+    worst = 0.0
+    for lo in range(0, 1 << n, CHUNK):
+        hi = min(lo + CHUNK, 1 << n)
+        w = qft_chunk(n, x, lo, hi)
+        g = got[lo:hi].astype(np.complex128)
+        ov += np.vdot(w, g)
+        nrm += float(np.vdot(g, g).real)
+        worst = max(worst, float(np.abs(g - w).max()))
+    gap = 1.0 - abs(ov) ** 2 / nrm
+    assert gap < 1e-6, gap
+    assert worst < 1e-4 * amp, (worst, amp)
+    assert abs(res["norm"] - 1.0) < 1e-5
