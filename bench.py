@@ -647,6 +647,32 @@ def workload_batched(args, dist, sq):
     return line
 
 
+def gate_layers_hbm(sq, n, prec, peak, peak_kind, cases=("hadamard_layer", "random_layers_2")):
+    """Short gate-layer measurements on one large state: one H layer on every qubit and two random Rz/Ry+CNOT
+    layers, each timed once with CUDA events after one untimed run; per-pass HBM GB/s as a fraction of the
+    peak (a pass reads and writes the state once)."""
+    wl = _workloads()
+    st = sq.State(n, prec).set_basis(0)
+    S = st.nbytes
+    out = {"qubits": n, "precision": prec, "state_bytes": S, "peak": peak, "peak_source": peak_kind}
+    for name in cases:
+        spec = wl.hadamard_benchmark(n, 1) if name == "hadamard_layer" else wl.random_layered(n, 2, seed=77)
+        plan = sq.Plan(spec.build(sq.Circuit()), n, prec)
+        st.execute(plan)
+        sq.synchronize()
+        with sq.Timer() as t:
+            st.execute(plan)
+        passes = plan.stats()["passes"]
+        gbs = passes * 2 * S / (t.ms * 1e-3) / 1e9
+        layers = 1 if name == "hadamard_layer" else 2
+        out[name] = {"ms": round(t.ms, 3), "passes": passes, "layers_per_s": round(layers / (t.ms * 1e-3), 3),
+                     "GB/s": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    norm = st.norm()
+    out["norm_after"] = norm
+    st.free()
+    return out
+
+
 def ref_run_request(spec, prec, threads):
     """Runs one circuit on the reference's own engine the way its algorithm libraries do
     (src/algorithms/lib_general.cpp:30-36, lib_grover.cpp:30-59): a DGM with its state allocated,
@@ -828,6 +854,9 @@ def workload_served(args, dist, sq):
     line["gpu_launches"] = launches
     line["clocks"] = clocks
     line["roofline"] = served_roofline(sq, args, peak, peak_kind)
+    if not args.skip_layers:
+        line["gate_layers_30q_f64"] = gate_layers_hbm(sq, 30, "f64", peak, peak_kind)
+        line["layered_32q_f32"] = gate_layers_hbm(sq, 32, "f32", peak, peak_kind, cases=("random_layers_2",))
     line["e2e"] = e2e
     if dist.rank == 0 and not args.skip_cpu:
         line["cpu_baseline"] = cpu_baseline_served(args, steps_reqs[args.warmup])
@@ -903,11 +932,11 @@ def cpu_baseline_served(args, reqs, budget_s=20.0):
     threads = os.cpu_count() or 1
     if not cpu.ref_available("f32"):
         return None
-    specs = [spec for spec, _ in reqs]
+    specs = [spec for spec, _ in reqs][::4]
     done, spent, _, _ = ref_stream(specs, "f32", threads, budget_s)
     return {"value": round(done / spent, 6), "unit": "circuits/s", "cores": threads, "kind": "reference",
-            "sample": f"the first {done} requests of the timed stream on t_PAR_CPU FP32, each unscaled, one "
-                      f"setFunction + execute per request ({spent:.1f} s)"}
+            "sample": f"every 4th request of the first timed step, the first {done} of them, on t_PAR_CPU FP32, "
+                      f"each unscaled, one setFunction + execute per request ({spent:.1f} s)"}
 
 
 WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": workload_grover,
@@ -1047,6 +1076,8 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-sweep", action="store_true", help="served: no Poisson rate sweep")
+    ap.add_argument("--skip-layers", action="store_true",
+                    help="served: no 30-qubit FP64 / 32-qubit FP32 gate-layer measurements")
     ap.add_argument("--qubits", type=int, default=0, help="override the workload's qubit count (profiling runs)")
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")

@@ -92,9 +92,15 @@ typedef struct hgm_plan_opts {
     int precision;   /* HGM_F64 / HGM_F32 */
     int warp_bits;   /* tile = 2^(10+warp_bits) amplitudes; -1 = default */
     int low_bits;    /* contiguous low index bits kept in every tile; -1 = default */
-    int fuse;        /* 1 = fuse adjacent gates on the same target and controls */
+    int fuse;        /* 1 = fuse adjacent gates on the same target and controls,
+                        except a pure phase next to a real gate (kept apart:
+                        the real gate takes the cheaper real form and the
+                        phase joins a phase block); 2 = fuse those too;
+                        0 = no fusion */
     int window;      /* scheduling look-ahead in ops; <=0 = default */
     int renorm_every;/* FP32: rescale to unit norm every k passes (0 = never) */
+    int chained;     /* 1 (default): a state of at most 32 MiB runs all its passes
+                        in one persistent launch; 0: one launch per pass */
 } hgm_plan_opts;
 
 void hgm_plan_default_opts(hgm_plan_opts *o, int precision);
@@ -138,8 +144,17 @@ int hgm_state_download(const hgm_state *s, void *host, int64_t bytes);
 
 /* ---- execution ---------------------------------------------------------- */
 
-/* Applies the plan `iterations` times on `stream` (0 = the library stream). */
+/* Applies the plan `iterations` times on `stream` (0 = the library stream).
+ * A state of at most 32 MiB (22 qubits FP32, 21 FP64) runs every pass in
+ * one persistent launch instead of one launch per pass; that launch's
+ * passes wait on each other with a bounded wait (hgm_plan_status).  The
+ * chained run's counters and an FP32 plan's renormalisation slots belong to
+ * the plan: executions of one plan must not overlap on the device. */
 int hgm_execute(hgm_state *s, const hgm_plan *p, int iterations, void *stream);
+/* After the plan's executions have been queued: waits for the device, then
+ * HGM_ERR_TIMEOUT if the last chained execution of the plan gave up a wait
+ * (its result is then not valid), else HGM_OK. */
+int hgm_plan_status(const hgm_plan *p);
 
 /* ---- device-resident measurement (FP64 reductions) ---------------------- */
 

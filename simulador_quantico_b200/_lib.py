@@ -37,7 +37,7 @@ class Result(C.Structure):
 
 class PlanOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("warp_bits", C.c_int), ("low_bits", C.c_int), ("fuse", C.c_int),
-                ("window", C.c_int), ("renorm_every", C.c_int)]
+                ("window", C.c_int), ("renorm_every", C.c_int), ("chained", C.c_int)]
 
 
 def _load():
@@ -78,6 +78,7 @@ def _load():
         "hgm_state_upload": ([vp, vp, i64], i),
         "hgm_state_download": ([vp, vp, i64], i),
         "hgm_execute": ([vp, vp, i, vp], i),
+        "hgm_plan_status": ([vp], i),
         "hgm_norm": ([vp, P(d)], i),
         "hgm_prob_one": ([vp, i, P(d)], i),
         "hgm_measure_qubit": ([vp, i, d, P(i), P(d)], i),

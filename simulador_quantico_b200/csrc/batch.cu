@@ -265,6 +265,7 @@ int batch_finalize(Batch *b) {
         hgm_plan_opts o;
         hgm_plan_default_opts(&o, b->precision);
         o.renorm_every = 0;
+        o.chained = 0;  // the batch kernel runs the passes itself
         o.warp_bits = b->warp_bits;
         o.low_bits = b->low_bits;
         j.plan.reset(new Plan());

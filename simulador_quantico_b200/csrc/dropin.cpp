@@ -10,12 +10,18 @@
 // back in place and the same pointer is returned; any failure prints a
 // message and exits with status 1 (kernel.cu:439-447).  Unlike the
 // reference, the device buffer is kept between calls of the same size and
-// precision (one cudaMalloc per process instead of one per call).
+// precision (one cudaMalloc per process instead of one per call), and the
+// plans of the last few PT lists are kept: a call whose list has the same
+// targets, controls and matrices as a cached one (compared in full, not by
+// hash alone) runs that plan instead of planning the list again.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <vector>
 
 #include "hgm_b200.h"
 #include "hgm_dropin.h"
@@ -54,10 +60,75 @@ hgm_state *state_for(int qubits) {
     return st;
 }
 
+// Plans of recent PT lists, keyed by the list's content: per PT its target
+// bit, control mask and value and its four matrix entries, as bytes.
+constexpr size_t kPlanCache = 8;
+struct CachedPlan {
+    int qubits = 0;
+    uint64_t hash = 0;
+    std::vector<unsigned char> key;
+    hgm_plan *plan = nullptr;
+    uint64_t last_use = 0;
+};
+std::vector<CachedPlan> g_plans;
+uint64_t g_use = 0;
+
+void pt_key(hgm_ref_pt **pts, std::vector<unsigned char> &key, uint64_t &hash) {
+    key.clear();
+    for (long i = 0; pts[i] != nullptr; i++) {
+        const hgm_ref_pt *pt = pts[i];
+        const size_t at = key.size();
+        key.resize(at + sizeof(int) + 2 * sizeof(long) + 4 * sizeof(hgm_dropin_amp));
+        unsigned char *d = key.data() + at;
+        memcpy(d, &pt->target_bit, sizeof(int));
+        memcpy(d + sizeof(int), &pt->control_mask, sizeof(long));
+        memcpy(d + sizeof(int) + sizeof(long), &pt->control_value, sizeof(long));
+        memcpy(d + sizeof(int) + 2 * sizeof(long), pt->matrix, 4 * sizeof(hgm_dropin_amp));
+    }
+    uint64_t h = 1469598103934665603ull;  // FNV-1a
+    for (unsigned char c : key) {
+        h ^= c;
+        h *= 1099511628211ull;
+    }
+    hash = h;
+}
+
+hgm_plan *plan_for(hgm_ref_pt **pts, int qubits);
+
 [[noreturn]] void die(const char *what) {
     printf("hgm_b200: %s: %s\n", what, hgm_last_error());
     fflush(stdout);
     exit(1);
+}
+
+hgm_plan *plan_for(hgm_ref_pt **pts, int qubits) {
+    static std::vector<unsigned char> key;
+    uint64_t hash = 0;
+    pt_key(pts, key, hash);
+    for (CachedPlan &c : g_plans)
+        if (c.qubits == qubits && c.hash == hash && c.key == key) {
+            c.last_use = ++g_use;
+            return c.plan;
+        }
+    hgm_plan_opts opts;
+    hgm_plan_default_opts(&opts, kPrecision);
+    hgm_plan *plan = nullptr;
+    if (hgm_plan_create_from_ref_pts(reinterpret_cast<void *const *>(pts), kPrecision, qubits, &opts, &plan))
+        die("planning");
+    if (g_plans.size() >= kPlanCache) {
+        auto old = std::min_element(g_plans.begin(), g_plans.end(),
+                                    [](const CachedPlan &a, const CachedPlan &b) { return a.last_use < b.last_use; });
+        hgm_plan_free(old->plan);  // waits for the device before freeing
+        g_plans.erase(old);
+    }
+    CachedPlan c;
+    c.qubits = qubits;
+    c.hash = hash;
+    c.key = key;
+    c.plan = plan;
+    c.last_use = ++g_use;
+    g_plans.push_back(std::move(c));
+    return plan;
 }
 
 }  // namespace
@@ -96,18 +167,14 @@ hgm_dropin_amp *GpuExecutionWrapper(hgm_dropin_amp *read_memory, hgm_ref_pt **pt
     }
     if (pts == nullptr) die("null PT list");
 
-    hgm_plan_opts opts;
-    hgm_plan_default_opts(&opts, kPrecision);
-    hgm_plan *plan = nullptr;
-    if (hgm_plan_create_from_ref_pts(reinterpret_cast<void *const *>(pts), kPrecision, qubits, &opts, &plan))
-        die("planning");
+    hgm_plan *plan = plan_for(pts, qubits);
     hgm_state *state = state_for(qubits);
     if (!state) die("state allocation");
     const int64_t bytes = (int64_t(1) << qubits) * (int64_t)sizeof(hgm_dropin_amp);
     if (hgm_state_upload(state, read_memory, bytes)) die("copy to device");
     if (hgm_execute(state, plan, iterations, nullptr)) die("execution");
     if (hgm_state_download(state, read_memory, bytes)) die("copy to host");
-    hgm_plan_free(plan);
+    if (hgm_plan_status(plan)) die("execution");  // a chained run that gave up a bounded wait
 
     if (debug) {
         double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();

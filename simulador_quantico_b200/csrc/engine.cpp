@@ -82,6 +82,7 @@ void hgm_plan_default_opts(hgm_plan_opts *o, int precision) {
     o->fuse = 1;
     o->window = 0;
     o->renorm_every = precision == HGM_F32 ? 64 : 0;
+    o->chained = 1;
 }
 
 static int finish_plan(const std::vector<Op> &ops, int qubits, const hgm_plan_opts *opts, hgm_plan **out) {
@@ -215,7 +216,22 @@ int hgm_execute(hgm_state *s, const hgm_plan *p, int iterations, void *stream) {
     int rc = upload_plan(pl);
     if (rc) return rc;
     if (iterations == 0) return HGM_OK;
+    // a state that fits in L2 runs every pass in one chained launch
+    if (plan_launches(pl, iterations) > 1 && chain_eligible(pl, iterations))
+        return launch_plan_chain(reinterpret_cast<State *>(s), pl, iterations, stream);
     return launch_plan(reinterpret_cast<State *>(s), pl, iterations, stream);
+}
+
+int hgm_plan_status(const hgm_plan *p) {
+    if (!p) return fail(HGM_ERR_INVALID, "null plan");
+    const Plan *pl = reinterpret_cast<const Plan *>(p);
+    const void *w = chain_error_word(pl);
+    if (!w) return HGM_OK;
+    uint64_t err = 0;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&err, w, sizeof err, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "plan status");
+    return err ? fail(HGM_ERR_TIMEOUT, "a chained pass gave up waiting for the passes before it") : HGM_OK;
 }
 
 int hgm_norm(hgm_state *s, double *out) {

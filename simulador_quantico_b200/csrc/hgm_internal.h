@@ -199,14 +199,26 @@ struct Plan {
     int64_t n_ops = 0, n_transposes = 0;
     // device copies, and their sizes as allocated
     DevAllocator *allocator = nullptr;
-    size_t d_bytes[4] = {0, 0, 0, 0};  // ops, phases, layouts, norm
+    size_t d_bytes[6] = {0, 0, 0, 0, 0, 0};  // ops, phases, layouts, norm, chain scratch, chain passes
     void *d_phases = nullptr;
     void *d_layouts = nullptr;
     void *d_ops = nullptr;
     int renorm_every = 0;
     double *d_norm = nullptr;         // renormalisation scratch (FP32 plans)
+    // Chained execution (launch_plan_chain), set up at upload for states of
+    // at most CHAIN_MAX_BYTES: the pass records on the device and the
+    // scratch (counters, error word, chain_slots renormalisation slots).
+    void *d_chain = nullptr;
+    void *d_chain_passes = nullptr;
+    int64_t chain_slots = 0;
+    bool chained = true;              // hgm_plan_opts.chained
     ~Plan();
 };
+
+// States up to this size run their passes chained in one launch (they fit
+// in L2 many times over, so a pass lasts a few microseconds and per-pass
+// launches would dominate).
+constexpr int64_t CHAIN_MAX_BYTES = int64_t(32) << 20;
 
 // Synchronous copy of a state between host and device memory (hostcopy.cpp):
 // large copies go through page-locked staging chunks on several threads.
@@ -239,6 +251,13 @@ struct PlanCursor {
 };
 int launch_plan_steps(State *s, const Plan *p, int iterations, PlanCursor *c, int64_t max_launches, void *stream);
 int64_t plan_launches(const Plan *p, int iterations);
+// The whole pass sequence of `iterations` runs of the plan in one persistent
+// launch (kernels.cu chain_kernel); only for plans chain_eligible() accepts.
+bool chain_eligible(const Plan *p, int iterations);
+int launch_plan_chain(State *s, const Plan *p, int iterations, void *stream);
+// Device address of the error word the last chained run of p set (nonzero:
+// a bounded wait gave up), for an asynchronous copy behind the run.
+const void *chain_error_word(const Plan *p);
 int launch_set_basis(State *s, int64_t index, void *stream);
 int reduce_norm(State *s, double *out, void *stream);
 int reduce_prob_one(State *s, int bit, double *out, void *stream);

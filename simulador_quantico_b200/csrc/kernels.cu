@@ -222,6 +222,158 @@ int64_t plan_launches(const Plan *p, int iterations) {
     return p->small ? 1 : (int64_t)p->passes.size() * iterations;
 }
 
+// ---------------------------------------------------------------------------
+// chained passes: every pass of a small state in one persistent launch
+// ---------------------------------------------------------------------------
+// A state that fits in L2 moves through a pass in a few microseconds, so
+// launching one kernel per pass leaves it bound by launch latency and the
+// tail of each launch.  The chained kernel runs the whole pass sequence in
+// one launch.  Its CTAs claim work items (pass g, tile t) in sequence order
+// from a counter, and the CTA that claimed an item of pass g waits until
+// every item of passes 0..g-1 is done (a second counter) before it loads.
+// An item only waits for items claimed before it, and a claimed item is held
+// by a running CTA, so the sequence always progresses whether or not all of
+// the grid is resident.  The wait is bounded (2 s of %globaltimer); a CTA
+// that gives up sets the error word and skips its tile.
+//
+// Scratch (Plan::d_chain): claim counter, done counter, error word, one
+// unused word, then one FP64 norm slot per renormalisation of the sequence.
+constexpr unsigned long long CHAIN_WAIT_LIMIT_NS = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long chain_now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <typename Real, int R, int W>
+__global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()))
+    chain_kernel(typename V2<Real>::T *__restrict__ state, const PassArgs *__restrict__ passes, int npasses,
+                 int tile_bits, long long total, int renorm, unsigned long long *ctr, double *norms) {
+    using A2 = typename V2<Real>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    A2 *sm = reinterpret_cast<A2 *>(smem_raw);
+    __shared__ long long s_item;
+    __shared__ int s_skip;
+    const long long seq = total >> tile_bits;  // passes in the sequence
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long it = (long long)atomicAdd(&ctr[0], 1ull);
+            s_item = it;
+            s_skip = 0;
+            if (it < total) {
+                const unsigned long long need = (unsigned long long)((it >> tile_bits) << tile_bits);
+                const unsigned long long t0 = chain_now_ns();
+                while (ld_acquire_u64(&ctr[1]) < need) {
+                    if (chain_now_ns() - t0 > CHAIN_WAIT_LIMIT_NS) {
+                        atomicExch(&ctr[2], 1ull);
+                        s_skip = 1;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __syncthreads();
+        const long long it = s_item;
+        if (it >= total) break;
+        if (!s_skip) {
+            const long long g = it >> tile_bits;
+            int32_t flags = 0;
+            double *norm_out = nullptr;
+            const double *scale_in = nullptr;
+            if (renorm > 0) {
+                // the plain launcher's schedule: a norm on every renorm-th
+                // pass but the last, a rescale on the pass after it
+                if ((g + 1) % renorm == 0 && g + 1 < seq) {
+                    flags |= PASS_NORM;
+                    norm_out = norms + ((g + 1) / renorm - 1);
+                }
+                if (g > 0 && g % renorm == 0) {
+                    flags |= PASS_SCALE;
+                    scale_in = norms + (g / renorm - 1);
+                }
+            }
+            run_tile<Real, R, W>(state, passes[g % npasses], (uint64_t)(it & ((1ll << tile_bits) - 1)), sm, flags,
+                                 norm_out, scale_in);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&ctr[1], 1ull);
+        }
+    }
+}
+
+template <typename Real, int R, int W>
+static int launch_chain_rw(State *s, const Plan *p, int iterations, cudaStream_t st) {
+    using A2 = typename V2<Real>::T;
+    static int grid_cap = 0;
+    const int smem = tile_smem_elems<R, W>() * (int)sizeof(A2);
+    if (!grid_cap) {
+        cudaError_t e = cudaFuncSetAttribute(chain_kernel<Real, R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int per_sm = 0, dev = 0, sms = 0;
+        if (e == cudaSuccess) e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel<Real, R, W>, 32 << W, smem);
+        if (e != cudaSuccess || per_sm < 1) return fail(HGM_ERR_CUDA, "chain kernel setup: %s", cudaGetErrorString(e));
+        grid_cap = sms * per_sm;
+    }
+    const int tile_bits = p->qubits - p->passes[0].k;
+    const long long total = ((long long)p->passes.size() * iterations) << tile_bits;
+    const long long ntiles = 1ll << tile_bits;
+    const unsigned grid = (unsigned)(ntiles < grid_cap ? ntiles : grid_cap);
+    unsigned long long *ctr = reinterpret_cast<unsigned long long *>(p->d_chain);
+    double *norms = reinterpret_cast<double *>(ctr + 4);
+    cudaError_t e = cudaMemsetAsync(p->d_chain, 0, p->d_bytes[4], st);
+    if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "chain scratch reset: %s", cudaGetErrorString(e));
+    chain_kernel<Real, R, W><<<grid, 32 << W, smem, st>>>(reinterpret_cast<A2 *>(s->d),
+                                                          reinterpret_cast<const PassArgs *>(p->d_chain_passes),
+                                                          (int)p->passes.size(), tile_bits, total, p->renorm_every,
+                                                          ctr, norms);
+    count_launch();
+    return check("chain_kernel launch");
+}
+
+template <typename Real>
+static int launch_chain_w(State *s, const Plan *p, int iterations, cudaStream_t st) {
+    constexpr int R = sizeof(Real) == 8 ? 4 : 5;
+    switch (p->warp_bits) {
+        case 0: return launch_chain_rw<Real, R, 0>(s, p, iterations, st);
+        case 1: return launch_chain_rw<Real, R, 1>(s, p, iterations, st);
+        case 2: return launch_chain_rw<Real, R, 2>(s, p, iterations, st);
+        default: return launch_chain_rw<Real, R, 3>(s, p, iterations, st);
+    }
+}
+
+bool chain_eligible(const Plan *p, int iterations) {
+    if (p->small || !p->d_chain || p->passes.size() < 2 || iterations < 1) return false;
+    const int64_t seq = (int64_t)p->passes.size() * iterations;
+    return p->renorm_every <= 0 || seq / p->renorm_every <= p->chain_slots;
+}
+
+int launch_plan_chain(State *s, const Plan *p, int iterations, void *stream) {
+    if (s->qubits != p->qubits || s->precision != p->precision)
+        return fail(HGM_ERR_INVALID, "plan and state differ in size or precision");
+    if (!chain_eligible(p, iterations)) return fail(HGM_ERR_INVALID, "plan not set up for chained passes");
+    cudaStream_t st = pick(stream);
+    if (!st) return HGM_ERR_CUDA;
+    return p->precision == HGM_F64 ? launch_chain_w<double>(s, p, iterations, st)
+                                   : launch_chain_w<float>(s, p, iterations, st);
+}
+
+// Error word of the last chained run of `p` (device address, for an
+// asynchronous copy after the run).
+const void *chain_error_word(const Plan *p) {
+    return p->d_chain ? reinterpret_cast<const unsigned long long *>(p->d_chain) + 2 : nullptr;
+}
+
 int launch_plan(State *s, const Plan *p, int iterations, void *stream) {
     PlanCursor c;
     return launch_plan_steps(s, p, iterations, &c, plan_launches(p, iterations), stream);
@@ -237,8 +389,8 @@ static cudaError_t plan_alloc(Plan *p, int k, void **out, size_t bytes) {
 }
 
 Plan::~Plan() {
-    void *ptrs[4] = {d_ops, d_phases, d_layouts, d_norm};
-    for (int k = 0; k < 4; k++) {
+    void *ptrs[6] = {d_ops, d_phases, d_layouts, d_norm, d_chain, d_chain_passes};
+    for (int k = 0; k < 6; k++) {
         if (!ptrs[k]) continue;
         if (allocator) allocator->free(ptrs[k], d_bytes[k]);
         else cudaFree(ptrs[k]);
@@ -293,6 +445,25 @@ int upload_plan(Plan *p) {
         pa.phases = reinterpret_cast<const DevPhase *>(p->d_phases);
         pa.layouts = reinterpret_cast<const uint32_t *>(p->d_layouts);
         pa.ops = p->d_ops;
+    }
+    const int64_t state_bytes = (int64_t(1) << p->qubits) * (p->precision == HGM_F64 ? 16 : 8);
+    if (p->chained && !p->small && p->passes.size() >= 2 && state_bytes <= CHAIN_MAX_BYTES) {
+        // chained execution: the pass records (pointers patched) and the scratch
+        p->chain_slots = p->renorm_every > 0 ? (int64_t)p->passes.size() / p->renorm_every + 1 : 0;
+        const size_t sb = (4 + (size_t)p->chain_slots) * sizeof(double);
+        const size_t pb = p->passes.size() * sizeof(PassArgs);
+        if ((e = plan_alloc(p, 4, &p->d_chain, sb)) != cudaSuccess)
+            return fail(HGM_ERR_NOMEM, "plan chain scratch: %s", cudaGetErrorString(e));
+        if ((e = plan_alloc(p, 5, &p->d_chain_passes, pb)) != cudaSuccess)
+            return fail(HGM_ERR_NOMEM, "plan chain passes: %s", cudaGetErrorString(e));
+        std::vector<PassArgs> dev(p->passes);
+        for (PassArgs &pa : dev) {
+            pa.flags = 0;
+            pa.norm_out = nullptr;
+            pa.scale_in = nullptr;
+        }
+        if ((e = cudaMemcpy(p->d_chain_passes, dev.data(), pb, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(HGM_ERR_CUDA, "plan chain passes copy: %s", cudaGetErrorString(e));
     }
     return HGM_OK;
 }

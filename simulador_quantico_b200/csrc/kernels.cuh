@@ -929,18 +929,23 @@ __device__ __forceinline__ void store_tile(const typename V2<Real>::T (&a)[1 << 
 // pass's load layout) and stores it.  `prev_cross`: the CTA's previous use
 // of `sm` may still be read by other warps, so the first transpose must
 // synchronise the CTA before writing.
+// flags, norm_out, scale_in: the pass's PASS_* flags and renormalisation
+// slots (the plain pass kernel passes pa's own; the chained kernel computes
+// them per position in the pass sequence).  The scale is read through L2:
+// in a chained run it was accumulated by other CTAs of the same launch.
 template <typename Real, int R, int W>
 __device__ __forceinline__ void finish_tile(typename V2<Real>::T (&a)[1 << R], typename V2<Real>::T *__restrict__ state,
                                             const PassArgs &pa, uint64_t base, typename V2<Real>::T *sm,
-                                            bool prev_cross) {
+                                            bool prev_cross, int32_t flags, double *norm_out,
+                                            const double *scale_in) {
     using A2 = typename V2<Real>::T;
     constexpr uint32_t LS = LAYOUT_HDR + (32u << W);  // words per layout table
     const uint32_t thr = threadIdx.x, lane = thr & 31;
     const DevOp<Real> *__restrict__ ops = reinterpret_cast<const DevOp<Real> *>(pa.ops);
     unsigned char *smb = reinterpret_cast<unsigned char *>(sm);
     int cur = pa.load_layout;
-    if (pa.flags & PASS_SCALE) {
-        const Real s = (Real)rsqrt(*pa.scale_in);
+    if (flags & PASS_SCALE) {
+        const Real s = (Real)rsqrt(__ldcg(scale_in));
 #pragma unroll
         for (int r = 0; r < (1 << R); r++) {
             a[r].x *= s;
@@ -971,13 +976,13 @@ __device__ __forceinline__ void finish_tile(typename V2<Real>::T (&a)[1 << R], t
         xr = 0;
     }
     store_tile<Real, R, W>(a, state, pa, base, xr);
-    if (pa.flags & PASS_NORM) {
+    if (flags & PASS_NORM) {
         double acc = 0.0;
 #pragma unroll
         for (int r = 0; r < (1 << R); r++) acc += (double)a[r].x * a[r].x + (double)a[r].y * a[r].y;
 #pragma unroll
         for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) atomicAdd(pa.norm_out, acc);
+        if (lane == 0) atomicAdd(norm_out, acc);
     }
 }
 
@@ -985,12 +990,18 @@ __device__ __forceinline__ void finish_tile(typename V2<Real>::T (&a)[1 << R], t
 // batched persistent kernel.
 template <typename Real, int R, int W>
 __device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ state, const PassArgs &pa, uint64_t tile,
-                                         typename V2<Real>::T *sm) {
+                                         typename V2<Real>::T *sm, int32_t flags, double *norm_out,
+                                         const double *scale_in) {
     using A2 = typename V2<Real>::T;
     const uint64_t base = tile_base(tile, pa);
     A2 a[1 << R];
     load_tile<Real, R, W>(a, state, pa, base, threadIdx.x);
-    finish_tile<Real, R, W>(a, state, pa, base, sm, false);
+    finish_tile<Real, R, W>(a, state, pa, base, sm, false, flags, norm_out, scale_in);
+}
+template <typename Real, int R, int W>
+__device__ __forceinline__ void run_tile(typename V2<Real>::T *__restrict__ state, const PassArgs &pa, uint64_t tile,
+                                         typename V2<Real>::T *sm) {
+    run_tile<Real, R, W>(state, pa, tile, sm, pa.flags, pa.norm_out, pa.scale_in);
 }
 
 }  // namespace hgm

@@ -47,11 +47,24 @@ void matmul2(const cplx a[4], const cplx b[4], cplx out[4]) {  // out = a * b
     for (int k = 0; k < 4; k++) out[k] = r[k];
 }
 
+bool pure_phase_diag(const SOp &s) {
+    return s.mc == MC_DIAG && std::abs(std::abs(s.m[0]) - 1.0) < 1e-12 && std::abs(std::abs(s.m[3]) - 1.0) < 1e-12;
+}
+bool real_dense(const SOp &s) {
+    return s.mc == MC_DENSE && s.m[0].imag() == 0 && s.m[1].imag() == 0 && s.m[2].imag() == 0 &&
+           s.m[3].imag() == 0;
+}
+
 // Merges each gate into the previous gate on the same target with the same
 // controls when nothing touched those qubits in between (one record instead
 // of two: the per-record work of the pass kernel outweighs the arithmetic a
-// cheaper matrix form would save).
-std::vector<SOp> fuse_ops(const std::vector<Op> &ops, bool fuse) {
+// cheaper matrix form would save).  With fuse == 1 a pure-phase diagonal
+// next to a real dense gate (an Rz before an Ry) stays apart: their product
+// is a complex dense gate, 8 floating-point instructions per amplitude, while
+// apart the real gate takes 4 (2 as packed FP32 pairs) and the phase joins a
+// phase block, where the phases of a whole layer cost two sweeps of the
+// registers.  fuse == 2 merges every such pair.
+std::vector<SOp> fuse_ops(const std::vector<Op> &ops, int fuse) {
     std::vector<SOp> out;
     out.reserve(ops.size());
     int64_t last_touch[64];
@@ -65,7 +78,10 @@ std::vector<SOp> fuse_ops(const std::vector<Op> &ops, bool fuse) {
         s.mc = classify(s.m);
         if (fuse) {
             int64_t y = last_touch[op.target];
-            if (y >= 0 && out[y].target == s.target && out[y].cmask == s.cmask && out[y].cval == s.cval) {
+            const bool keep_apart = y >= 0 && fuse == 1 &&
+                                    ((pure_phase_diag(out[y]) && real_dense(s)) || (real_dense(out[y]) && pure_phase_diag(s)));
+            if (y >= 0 && !keep_apart && out[y].target == s.target && out[y].cmask == s.cmask &&
+                out[y].cval == s.cval) {
                 bool adjacent = true;
                 uint64_t sup = s.sup();
                 while (sup) {
@@ -724,7 +740,8 @@ int build_plan(const std::vector<Op> &ops, int n, const hgm_plan_opts &opts, Pla
     plan->precision = opts.precision;
     plan->qubits = n;
     plan->renorm_every = opts.precision == HGM_F32 ? opts.renorm_every : 0;
-    std::vector<SOp> sops = fuse_ops(ops, opts.fuse != 0);
+    plan->chained = opts.chained != 0;
+    std::vector<SOp> sops = fuse_ops(ops, opts.fuse);
     plan->n_ops = (int64_t)sops.size();
     // amplitudes per thread: 16 for FP64 (64 data registers), 32 for FP32
     const int R = opts.precision == HGM_F64 ? 4 : 5;

@@ -36,6 +36,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
@@ -88,8 +89,8 @@ struct Slot {
     bool tail = false;   // reductions and result copy queued (s.done recorded)
     double *partials = nullptr;
     long long *ibest = nullptr;
-    double *dres = nullptr;   // 4 doubles
-    double *hres = nullptr;   // pinned, 4 doubles
+    double *dres = nullptr;   // 4 doubles: norm (2 slots), argmax probability and index
+    double *hres = nullptr;   // pinned, 6 doubles: dres, then a chained run's error word
     Request *req = nullptr;
 };
 
@@ -150,9 +151,15 @@ struct StateCache {
 // cudaMalloc and cudaFree take the device's allocation lock and cudaFree
 // can wait on running work, so freeing a finished request's plan while
 // other slots run stalled them all; recycled blocks avoid both calls.
+// Every block it hands out is its own cudaMalloc of the class size, and a
+// block comes back only as the pointer and class it went out with (`live`
+// holds the blocks out): a pointer into the middle of a block, or one freed
+// twice, is refused rather than entered in a free list, where it would later
+// be handed out as a block overlapping a live one.
 struct PlanMemory : DevAllocator {
     std::mutex mu;
     std::map<size_t, std::vector<void *>> free_by_class;
+    std::map<void *, size_t> live;
     static size_t size_class(size_t b) {
         size_t c = 256;
         while (c < b) c <<= 1;
@@ -160,25 +167,33 @@ struct PlanMemory : DevAllocator {
     }
     cudaError_t alloc(void **p, size_t bytes) override {
         const size_t c = size_class(bytes);
-        {
-            std::lock_guard<std::mutex> lk(mu);
-            auto &v = free_by_class[c];
-            if (!v.empty()) {
-                *p = v.back();
-                v.pop_back();
-                return cudaSuccess;
-            }
+        std::lock_guard<std::mutex> lk(mu);
+        auto &v = free_by_class[c];
+        if (!v.empty()) {
+            *p = v.back();
+            v.pop_back();
+        } else {
+            cudaError_t e = cudaMalloc(p, c);
+            if (e != cudaSuccess) return e;
         }
-        return cudaMalloc(p, c);
+        live[*p] = c;
+        return cudaSuccess;
     }
     // The GPU must be done with the block.
     void free(void *p, size_t bytes) override {
         std::lock_guard<std::mutex> lk(mu);
+        auto it = live.find(p);
+        if (it == live.end() || it->second != size_class(bytes)) {
+            set_error("plan memory: a block was returned that this cache did not hand out");
+            return;
+        }
+        live.erase(it);
         free_by_class[size_class(bytes)].push_back(p);
     }
     ~PlanMemory() {
         for (auto &kv : free_by_class)
             for (void *p : kv.second) cudaFree(p);
+        for (auto &kv : live) cudaFree(kv.first);
     }
 };
 
@@ -247,6 +262,10 @@ struct Server {
         Request *r = s.req;
         r->t_done = now_s();
         r->norm = s.hres[0];
+        uint64_t chain_err = 0;
+        memcpy(&chain_err, s.hres + 4, sizeof chain_err);
+        if (chain_err && r->status == HGM_OK)
+            r->status = fail(HGM_ERR_TIMEOUT, "request %lld: a chained pass gave up waiting", (long long)r->id);
         if (r->result_mask) {
             r->pmax = s.hres[2];
             r->argmax = (int64_t)s.hres[3];
@@ -300,6 +319,7 @@ struct Server {
         s.total = plan_launches(r->plan, 1);
         s.chunks_in_flight = 0;
         s.tail = false;
+        s.hres[4] = 0.0;  // the error word of a chained run is copied here behind it
         int rc = launch_set_basis(&r->state, r->init_index, s.stream);
         return rc ? rc : feed(s);
     }
@@ -309,6 +329,14 @@ struct Server {
     int feed(Slot &s) {
         Request *r = s.req;
         while (!s.tail && s.chunks_in_flight < 2) {
+            if (s.cursor.next == 0 && s.total > 1 && chain_eligible(r->plan, 1)) {
+                // a small state: every pass in one persistent launch
+                int rc = launch_plan_chain(&r->state, r->plan, 1, s.stream);
+                if (rc) return rc;
+                cudaMemcpyAsync(s.hres + 4, chain_error_word(r->plan), sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                s.stream);
+                s.cursor.next = s.total;
+            }
             if (s.cursor.next < s.total) {
                 int rc = launch_plan_steps(&r->state, r->plan, 1, &s.cursor, kChunkLaunches, s.stream);
                 if (rc) return rc;
@@ -492,7 +520,7 @@ int hgm_server_create(const hgm_server_opts *opts, hgm_server **out) {
             (e = cudaMalloc(&sl.partials, 2 * REDUCE_SCRATCH_BLOCKS * sizeof(double))) != cudaSuccess ||
             (e = cudaMalloc(&sl.ibest, REDUCE_SCRATCH_BLOCKS * sizeof(long long))) != cudaSuccess ||
             (e = cudaMalloc(&sl.dres, 4 * sizeof(double))) != cudaSuccess ||
-            (e = cudaMallocHost(&sl.hres, 4 * sizeof(double))) != cudaSuccess)
+            (e = cudaMallocHost(&sl.hres, 6 * sizeof(double))) != cudaSuccess)
             return fail(HGM_ERR_CUDA, "server slot: %s", cudaGetErrorString(e));
     }
     cudaGetDevice(&s->device);

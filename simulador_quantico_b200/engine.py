@@ -122,6 +122,11 @@ class Plan:
         check(lib.hgm_plan_upload(self.h))
         return self
 
+    def status(self):
+        """Waits for the device; raises if the plan's last chained execution gave up a bounded wait."""
+        check(lib.hgm_plan_status(self.h))
+        return self
+
     def stats(self) -> dict:
         v = [C.c_int64() for _ in range(4)]
         check(lib.hgm_plan_stats(self.h, *[C.byref(x) for x in v]))

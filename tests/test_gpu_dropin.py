@@ -137,3 +137,24 @@ def test_wrapper_interleaved_sizes(sq):
         c = spec.build(__import__("oracle.circuit_lang", fromlist=["Circuit"]).Circuit())
         want = cpu.run_serial(init, n, c.as_arrays())
         assert np.abs(got - want).max() < TOL_F64, n
+
+
+def test_wrapper_plan_cache(sq):
+    """GpuExecutionWrapper keeps the plans of recent PT lists: the same list on
+    new inputs, a list of the same length with one matrix changed, and more
+    lists than the cache holds all give the oracle's results."""
+    n = 13
+    L = sq.load_dropin("f64")
+    assert L.setDevice(0) is False
+    specs = [random_gate_circuit_spec(n, 40, seed=900 + k) for k in range(10)]
+    twin = random_gate_circuit_spec(n, 40, seed=900)
+    first = next(iter(twin.gates))
+    twin.gates[first] = [0, 1j, 1j, 0]  # same targets and controls, another matrix
+    for rep in range(2):
+        for k, spec in enumerate(specs[:3] + [twin] + specs[3:]):
+            init = random_state(n, seed=rep * 100 + k)
+            c = spec.build(sq.Circuit())
+            host = init.copy()
+            L.GpuExecutionWrapper(host.ctypes.data, c.ref_pts("f64"), n, 4, 8, 1, 64, 2, 1)
+            want = oracle_state(spec, "f64", init=init)
+            assert np.abs(host - want).max() < TOL_F64, (rep, k)

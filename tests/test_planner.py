@@ -12,7 +12,7 @@ from tests.helpers import oracle_state, random_gate_circuit_spec, random_state
 
 @pytest.mark.parametrize("n", [5, 9, 10, 11, 12, 14])
 @pytest.mark.parametrize("warp_bits", [0, 1, 2, 3])
-@pytest.mark.parametrize("fuse", [0, 1])
+@pytest.mark.parametrize("fuse", [0, 1, 2])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_emulated_plan_matches_oracle(n, warp_bits, fuse, prec):
     R = emu.REG_BITS[prec]
@@ -82,13 +82,17 @@ def test_plan_pass_counts():
     spec = wl.random_layered(30, 4, seed=1)
     p = sq.Plan(spec.build(sq.Circuit()), 30, "f64")
     s = p.stats()
-    assert s["ops"] == 4 * 45  # Rz.Ry fused per qubit + 15 CNOTs per layer
+    assert s["ops"] == 4 * 75  # Rz and Ry kept apart per qubit + 15 CNOTs per layer
     assert s["passes"] <= 4 * 3
+    p2 = sq.Plan(spec.build(sq.Circuit()), 30, "f64", fuse=2)
+    assert p2.stats()["ops"] == 4 * 45  # fuse=2: Rz.Ry merged per qubit
+    assert p2.stats()["passes"] <= 4 * 3
 
 
 def test_fusion_merges_adjacent():
-    """Adjacent gates on one target merge (H.H and Rz.Rz.Ry become one
-    record each); a gate on another qubit in between does not block it."""
+    """Adjacent gates on one target merge (H.H becomes one record, Rz.Rz.Ry
+    two: a pure phase next to a real gate stays apart by default, one record
+    with fuse=2); a gate on another qubit in between does not block it."""
     h = np.array([[1, 1], [1, -1]]) / np.sqrt(2)
 
     def rz(t):
@@ -105,7 +109,9 @@ def test_fusion_merges_adjacent():
     c = sq.Circuit()
     for m in (rz(0.3), rz(0.5), ry(0.7)):
         c.append_op(0, 0, 0, m)
-    assert sq.Plan(c, 12, "f64").stats()["ops"] == 1
+    # Rz.Rz merge; the pure phase and the real Ry stay apart unless fuse=2
+    assert sq.Plan(c, 12, "f64").stats()["ops"] == 2
+    assert sq.Plan(c, 12, "f64", fuse=2).stats()["ops"] == 1
 
 
 def test_grover_plan_fast():
@@ -144,7 +150,7 @@ def test_randomized_plans():
                     lambda: wl.grover_search(n, int(rng.integers(1 << n)), iterations=2)][kind]()
             init = np.zeros(1 << n, dtype=np.complex128)
             init[spec.init_index] = 1
-        plan = sq.Plan(spec.build(sq.Circuit()), n, prec, warp_bits=W, low_bits=lb, fuse=case % 3 != 0,
+        plan = sq.Plan(spec.build(sq.Circuit()), n, prec, warp_bits=W, low_bits=lb, fuse=case % 3,
                        renorm_every=0)
         got = emu.run(plan, prec, init)
         want = oracle_state(spec, "f64", init=init)
