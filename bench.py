@@ -673,18 +673,23 @@ def gate_layers_hbm(sq, n, prec, peak, peak_kind, cases=("hadamard_layer", "rand
     return out
 
 
-def ref_run_request(spec, prec, threads):
+def ref_run_request(spec, prec, threads, gpu=False):
     """Runs one circuit on the reference's own engine the way its algorithm libraries do
     (src/algorithms/lib_general.cpp:30-36, lib_grover.cpp:30-59): a DGM with its state allocated,
     setMemoryValue, the circuit's gates (Gates::addGate), one setFunction per call of the circuit and one
-    execute on t_PAR_CPU with `threads` OpenMP threads.  Returns the wall seconds of all of it."""
+    execute -- on t_PAR_CPU with `threads` OpenMP threads, or with gpu=True on t_GPU, the reference's own
+    kernel.cu built for sm_100a, with the CLIs' default GPU tuning (include/cli/cli_common.h:8-17).
+    Returns the wall seconds of all of it."""
     from oracle import cpu
 
     t0 = time.perf_counter()
-    r = cpu.RefDGM(spec.qubits, prec)
+    r = cpu.RefDGM(spec.qubits, prec, gpu=gpu)
     r.set_memory_value(spec.init_index)
     spec.build(r)
-    r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
+    if gpu:
+        r.tuning(cpu.RefDGM.T_GPU)
+    else:
+        r.tuning(cpu.RefDGM.T_PAR_CPU, thread_count=threads)
     r.execute(1)
     dt = time.perf_counter() - t0
     r.close()
@@ -1003,6 +1008,50 @@ def reference_stream_specs(args):
     return None, None
 
 
+def reference_gpu_leg(args):
+    """The reference's own t_GPU (kernel.cu for sm_100a, FP32, oracle/_ref/libref_gpu_f32.so) on the first
+    timed step's requests in order, each unscaled, for about args.ref_gpu_s seconds after one untimed
+    request.  Runs in a child process (`--impl reference-gpu`): the reference exits the process on any CUDA
+    error (src/core/kernel.cu:439-447)."""
+    from oracle import cpu
+
+    if not cpu.ref_available("f32", gpu=True):
+        return {"unavailable": "the reference's GPU backend (oracle/_ref/libref_gpu_f32.so) was not built"}
+    count = args.requests or 48
+    specs = [spec for spec, _ in served_requests(1000 + args.warmup, count)]
+    small = min(specs, key=lambda s: (s.qubits, s.n_ops_estimate()))
+    ref_run_request(small, "f32", 1, gpu=True)  # CUDA context and module load
+    done, spent, each = 0, 0.0, []
+    for spec in specs:
+        dt = ref_run_request(spec, "f32", 1, gpu=True)
+        each.append(dt)
+        spent += dt
+        done += 1
+        if spent >= args.ref_gpu_s:
+            break
+    return {"value": round(done / spent, 4), "unit": "circuits/s", "requests": done, "seconds": round(spent, 3),
+            "latency_ms": {"p50": round(float(np.percentile(each, 50)) * 1e3, 3),
+                           "p99": round(float(np.percentile(each, 99)) * 1e3, 3)},
+            "path": "the reference's DGM on t_GPU (GpuExecutionWrapper of its kernel.cu, built for sm_100a with "
+                    "max_target_bit initialised), default GPU tuning, host state per request",
+            "sample": f"the first {done} requests of the first timed step, in order, each unscaled"}
+
+
+def reference_gpu_in_child(args):
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference-gpu", "--requests", str(args.requests or 48),
+           "--warmup", str(args.warmup), "--ref-gpu-s", str(args.ref_gpu_s)]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR",
+                                                                "MASTER_PORT")}
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=args.ref_gpu_s * 4 + 120, env=env)
+        lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
+        if p.returncode == 0 and lines:
+            return json.loads(lines[-1])
+        return {"unavailable": f"child exited {p.returncode}: {(p.stdout + p.stderr).strip()[-300:]}"}
+    except Exception as e:
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
 def reference_arm(args, dist):
     """The reference's own CPU implementation (t_PAR_CPU, oracle/_ref), rank 0 only, with every host thread.
 
@@ -1056,6 +1105,8 @@ def reference_arm(args, dist):
                      "dtype": "f64"})
     line["cpu_baseline"] = {"value": line["value"], "unit": unit, "cores": threads, "kind": "reference",
                             "sample": sample}
+    if args.workload == "served" and not args.skip_ref_gpu:
+        line["reference_gpu"] = reference_gpu_in_child(args)
     line["e2e"] = {"value": line["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     return line
 
@@ -1072,7 +1123,10 @@ def main():
     ap.add_argument("--inflight", type=int, default=16, help="server slots")
     ap.add_argument("--plain-limit", type=float, default=60.0, help="seconds cap for the plain FP64 comparison")
     ap.add_argument("--skip-fidelity", action="store_true")
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"])
+    ap.add_argument("--ref-gpu-s", type=float, default=30.0,
+                    help="reference arm, served: seconds of the reference's own t_GPU leg")
+    ap.add_argument("--skip-ref-gpu", action="store_true", help="reference arm: no t_GPU leg")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-sweep", action="store_true", help="served: no Poisson rate sweep")
@@ -1092,6 +1146,8 @@ def main():
     try:
         if args.impl == "reference":
             line = reference_arm(args, dist)
+        elif args.impl == "reference-gpu":
+            line = reference_gpu_leg(args) if dist.rank == 0 else None
         else:
             import simulador_quantico_b200 as sq
 

@@ -92,10 +92,10 @@ typedef struct hgm_plan_opts {
     int precision;   /* HGM_F64 / HGM_F32 */
     int warp_bits;   /* tile = 2^(10+warp_bits) amplitudes; -1 = default */
     int low_bits;    /* contiguous low index bits kept in every tile; -1 = default */
-    int fuse;        /* 1 = fuse adjacent gates on the same target and controls,
-                        except a pure phase next to a real gate (kept apart:
-                        the real gate takes the cheaper real form and the
-                        phase joins a phase block); 2 = fuse those too;
+    int fuse;        /* 1 = fuse adjacent gates on the same target and
+                        controls; 2 = the same, except a pure phase next to a
+                        real gate (kept apart: the real gate takes the
+                        cheaper real form, the phase joins a phase block);
                         0 = no fusion */
     int window;      /* scheduling look-ahead in ops; <=0 = default */
     int renorm_every;/* FP32: rescale to unit norm every k passes (0 = never) */

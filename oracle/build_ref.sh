@@ -20,6 +20,10 @@
 #                               backend replaced at link time by
 #                               libhgm_dropin_{f32,f64}.so (only when those
 #                               exist)
+#   oracle/_ref/libref_gpu_f32.so
+#                               the unmodified FP32 core with the reference's
+#                               own GPU backend (src/core/kernel.cu) compiled
+#                               for sm_100a (one scripted fix, see below)
 #
 # Sources are read where they lie under the reference tree, whose root the
 # caller names in REF_ROOT (required; nothing is built without it); the widened copy is written to a scratch folder
@@ -91,6 +95,27 @@ build_variant() {
     $CXX -o "$OUT/general_ref_$prec.out" "$work/obj/general.o" $core "$work/obj/kernel_stub.o" -fopenmp
     $CXX -o "$OUT/grover_ref_$prec.out" "$work/obj/grover.o" $core "$work/obj/kernel_stub.o" -fopenmp
     $CXX -o "$OUT/shor_ref_$prec.out" "$work/obj/shor.o" $core "$work/obj/kernel_stub.o" -fopenmp
+
+    # The reference's own GPU backend (makefile:49-59, GPU=real), FP32 only
+    # (kernel.cu is written for cuFloatComplex), compiled for sm_100a with the
+    # makefile's kernel flags (makefile:26,93) and one scripted change:
+    # GpuExecution01 declares max_target_bit uninitialised (kernel.cu:206) and
+    # reads it at :235 when a batch holds only targets below coalesced_bits,
+    # so region_start_bit -- and every address of that launch -- would come
+    # from an indeterminate value.  It is initialised to 0 here, which keeps
+    # such a batch at region_start_bit = coalesced_bits, inside the state.
+    if [ "$prec" = "f32" ] && command -v "${NVCC:-nvcc}" > /dev/null; then
+        sed -i 's/int max_target_bit, min_target_bit = coalesced_bits;/int max_target_bit = 0, min_target_bit = coalesced_bits;/' \
+            "$work/src/core/kernel.cu"
+        grep -q "int max_target_bit = 0, min_target_bit" "$work/src/core/kernel.cu" || {
+            echo "build_ref.sh: kernel.cu patch did not apply" >&2
+            exit 1
+        }
+        "${NVCC:-nvcc}" -arch=sm_100a -O3 -D OPS_BLOCK=300 -Xcompiler -fPIC $inc -c "$work/src/core/kernel.cu" \
+            -o "$work/obj/kernel.o"
+        "${NVCC:-nvcc}" -arch=sm_100a -shared -o "$OUT/libref_gpu_$prec.so" $core "$work/obj/kernel.o" \
+            "$work/obj/ref_harness.o" -Xcompiler -fopenmp
+    fi
 
     # Link-time replacement of the GPU backend (makefile:51-61) by the
     # product's drop-in library, when it has been built.

@@ -118,9 +118,16 @@ def basis_state(qubits, index, dtype=np.complex128):
 
 # ---- the reference's own engine (built by oracle/build_ref.sh) ----------
 
-def ref_available(prec="f64", dropin=False):
-    name = f"libref_dropin_{prec}.so" if dropin else f"libref_{prec}.so"
-    return (REF / name).exists()
+def _ref_lib_name(prec, dropin=False, gpu=False):
+    if gpu:
+        return f"libref_gpu_{prec}.so"
+    return f"libref_dropin_{prec}.so" if dropin else f"libref_{prec}.so"
+
+
+def ref_available(prec="f64", dropin=False, gpu=False):
+    """dropin: the reference's objects linked against the product's drop-in;
+    gpu: linked with the reference's own GPU backend (kernel.cu, FP32 only)."""
+    return (REF / _ref_lib_name(prec, dropin, gpu)).exists()
 
 
 class RefDGM:
@@ -129,18 +136,17 @@ class RefDGM:
     T_CPU, T_PAR_CPU, T_GPU, T_HYBRID = 0, 1, 2, 3
     _libs: dict = {}
 
-    def __init__(self, qubits, prec="f64", dropin=False):
-        self.lib = self._load(prec, dropin)
+    def __init__(self, qubits, prec="f64", dropin=False, gpu=False):
+        self.lib = self._load(prec, dropin, gpu)
         self.qubits = qubits
         self.prec = prec
         self.h = self.lib.ref_dgm_new(qubits)
 
     @classmethod
-    def _load(cls, prec, dropin):
-        key = (prec, dropin)
+    def _load(cls, prec, dropin, gpu=False):
+        key = (prec, dropin, gpu)
         if key not in cls._libs:
-            name = f"libref_dropin_{prec}.so" if dropin else f"libref_{prec}.so"
-            L = C.CDLL(str(REF / name))
+            L = C.CDLL(str(REF / _ref_lib_name(prec, dropin, gpu)))
             L.ref_dgm_new.restype = C.c_void_p
             L.ref_dgm_new.argtypes = [C.c_int]
             L.ref_dgm_free.argtypes = [C.c_void_p]

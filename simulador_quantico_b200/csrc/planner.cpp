@@ -58,12 +58,14 @@ bool real_dense(const SOp &s) {
 // Merges each gate into the previous gate on the same target with the same
 // controls when nothing touched those qubits in between (one record instead
 // of two: the per-record work of the pass kernel outweighs the arithmetic a
-// cheaper matrix form would save).  With fuse == 1 a pure-phase diagonal
-// next to a real dense gate (an Rz before an Ry) stays apart: their product
-// is a complex dense gate, 8 floating-point instructions per amplitude, while
-// apart the real gate takes 4 (2 as packed FP32 pairs) and the phase joins a
-// phase block, where the phases of a whole layer cost two sweeps of the
-// registers.  fuse == 2 merges every such pair.
+// cheaper matrix form would save).  fuse == 2 keeps a pure-phase diagonal
+// next to a real dense gate (an Rz before an Ry) apart: the real gate then
+// takes 4 floating-point instructions per amplitude (2 as packed FP32 pairs)
+// instead of the product's 8, and the phase joins a phase block.  Measured
+// on 26-qubit FP32 and 30-qubit FP64 random layered circuits that is slower
+// (1.07 against 0.79 ms per FP32 pass; 19.2 against 30.9 FP64 layers/s): the
+// phase blocks' per-term work outweighs the arithmetic saved, so fuse == 1
+// merges every such pair.
 std::vector<SOp> fuse_ops(const std::vector<Op> &ops, int fuse) {
     std::vector<SOp> out;
     out.reserve(ops.size());
@@ -78,7 +80,7 @@ std::vector<SOp> fuse_ops(const std::vector<Op> &ops, int fuse) {
         s.mc = classify(s.m);
         if (fuse) {
             int64_t y = last_touch[op.target];
-            const bool keep_apart = y >= 0 && fuse == 1 &&
+            const bool keep_apart = y >= 0 && fuse == 2 &&
                                     ((pure_phase_diag(out[y]) && real_dense(s)) || (real_dense(out[y]) && pure_phase_diag(s)));
             if (y >= 0 && !keep_apart && out[y].target == s.target && out[y].cmask == s.cmask &&
                 out[y].cval == s.cval) {

@@ -52,7 +52,8 @@ def test_chained_iterations_and_renorm(sq):
     assert launches == 1 and passes > 64
     want = oracle_state(spec, "f64")
     assert np.abs(got - want).max() < 1e-4
-    assert abs(np.vdot(got, got).real - 1.0) < 1e-5
+    # renormalised every 64 passes: FP32 drift of at most 63 passes remains
+    assert abs(np.vdot(got.astype(np.complex128), got.astype(np.complex128)).real - 1.0) < 1e-4
     assert int(np.argmax(np.abs(got))) == w
     # a one-iteration plan run 4 times: the chained sequence spans the iterations
     it_spec = wl.grover_search(n, w, iterations=4)

@@ -77,17 +77,22 @@ def test_grover_search_26q_full(sq):
     got = st.download()
     st.free()
     marked, other = cf.grover_amplitudes(n, k)
-    # 334,542 Hadamard applications scale the norm by (2 h^2)^(1/2) each,
-    # h = 1/sqrt(2) rounded to FP64 -- a systematic drift any FP64 simulator of
-    # this circuit shares, the reference's CPU engine included; it stays
-    # bounded, and the state's direction matches the closed form to 1e-12
+    # 6433 iterations are about 400,000 gate applications (334,542 of them
+    # Hadamards with h = 1/sqrt(2) rounded to FP64).  Their rounding moved
+    # the marked amplitude by 3e-11 (measured), the normalised one by 4e-12:
+    # the same order for any FP64 simulator of this circuit, the reference's
+    # CPU engine included.  So the raw norm drift must stay below 1e-9 and the
+    # normalised state must match the closed form within 2e-11 (about 3e-15
+    # per iteration); the first iterations are held to 1e-12 against the
+    # oracle's engine, unnormalised, below.
     norm = float(np.vdot(got, got).real)
     assert abs(norm - 1.0) < 1e-9, norm
     unit = got / np.sqrt(norm)
-    assert abs(unit[mark] - marked) < TOL_F64
-    assert abs(p / norm - marked * marked) < 1e-12
+    tol_long = 2e-11
+    assert abs(unit[mark] - marked) < tol_long
+    assert abs(p / norm - marked * marked) < tol_long
     unit[mark] = other
-    assert np.abs(unit - other).max() < TOL_F64
+    assert np.abs(unit - other).max() < tol_long
 
 
 def test_grover_search_26q_vs_oracle(sq):

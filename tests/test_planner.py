@@ -82,17 +82,17 @@ def test_plan_pass_counts():
     spec = wl.random_layered(30, 4, seed=1)
     p = sq.Plan(spec.build(sq.Circuit()), 30, "f64")
     s = p.stats()
-    assert s["ops"] == 4 * 75  # Rz and Ry kept apart per qubit + 15 CNOTs per layer
+    assert s["ops"] == 4 * 45  # Rz.Ry fused per qubit + 15 CNOTs per layer
     assert s["passes"] <= 4 * 3
     p2 = sq.Plan(spec.build(sq.Circuit()), 30, "f64", fuse=2)
-    assert p2.stats()["ops"] == 4 * 45  # fuse=2: Rz.Ry merged per qubit
+    assert p2.stats()["ops"] == 4 * 75  # fuse=2: Rz and Ry kept apart
     assert p2.stats()["passes"] <= 4 * 3
 
 
 def test_fusion_merges_adjacent():
-    """Adjacent gates on one target merge (H.H becomes one record, Rz.Rz.Ry
-    two: a pure phase next to a real gate stays apart by default, one record
-    with fuse=2); a gate on another qubit in between does not block it."""
+    """Adjacent gates on one target merge (H.H and Rz.Rz.Ry become one record
+    each; with fuse=2 a pure phase next to a real gate stays apart); a gate on
+    another qubit in between does not block it."""
     h = np.array([[1, 1], [1, -1]]) / np.sqrt(2)
 
     def rz(t):
@@ -109,9 +109,9 @@ def test_fusion_merges_adjacent():
     c = sq.Circuit()
     for m in (rz(0.3), rz(0.5), ry(0.7)):
         c.append_op(0, 0, 0, m)
-    # Rz.Rz merge; the pure phase and the real Ry stay apart unless fuse=2
-    assert sq.Plan(c, 12, "f64").stats()["ops"] == 2
-    assert sq.Plan(c, 12, "f64", fuse=2).stats()["ops"] == 1
+    # all three merge; with fuse=2 the pure phase (Rz.Rz) and the real Ry stay apart
+    assert sq.Plan(c, 12, "f64").stats()["ops"] == 1
+    assert sq.Plan(c, 12, "f64", fuse=2).stats()["ops"] == 2
 
 
 def test_grover_plan_fast():
