@@ -239,7 +239,7 @@ void batch_launch(Batch *b, cudaStream_t st) {
 
 template <typename Real>
 int batch_dispatch(Batch *b, bool setup, cudaStream_t st) {
-    constexpr int R = sizeof(Real) == 8 ? 4 : 5;
+    constexpr int R = sizeof(Real) == 8 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS;
     switch (b->warp_bits) {
         case 0: return setup ? batch_setup<Real, R, 0>(b) : (batch_launch<Real, R, 0>(b, st), HGM_OK);
         case 1: return setup ? batch_setup<Real, R, 1>(b) : (batch_launch<Real, R, 1>(b, st), HGM_OK);
@@ -256,7 +256,7 @@ int cuda_err(cudaError_t e, const char *what) {
 int batch_finalize(Batch *b) {
     if (b->finalized) return HGM_OK;
     if (b->jobs.empty()) return fail(HGM_ERR_INVALID, "empty batch");
-    const int R = b->precision == HGM_F64 ? 4 : 5;
+    const int R = reg_bits_for(b->precision);
     const int K = 5 + R + b->warp_bits;
     const size_t amp = b->precision == HGM_F64 ? 16 : 8;
     // plans and arena layout

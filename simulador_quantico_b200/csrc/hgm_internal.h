@@ -135,6 +135,17 @@ struct DevPhase {
     int32_t xwarp;   // 1 if entering this phase needs a cross-warp transpose
 };
 
+// Amplitudes a thread keeps in registers, 2^R: R = HGM_F64_REG_BITS for
+// FP64 (16 double2 by default) and HGM_F32_REG_BITS for FP32 (32 float2 by
+// default).
+#ifndef HGM_F32_REG_BITS
+#define HGM_F32_REG_BITS 5
+#endif
+#ifndef HGM_F64_REG_BITS
+#define HGM_F64_REG_BITS 4
+#endif
+constexpr int reg_bits_for(int precision) { return precision == HGM_F64 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS; }
+
 constexpr int MAX_TILE_BITS = 16;
 // Runs of consecutive non-tile index bits: at most one more than tile bits.
 constexpr int MAX_FREE_RUNS = MAX_TILE_BITS + 2;

@@ -154,7 +154,7 @@ static int launch_pass(void *state, const PassArgs &pa, cudaStream_t st) {
 // FP64 tiles hold 16 amplitudes a thread (R = 4), FP32 tiles 32 (R = 5).
 template <typename Real>
 static int launch_pass_w(int W, void *state, const PassArgs &pa, cudaStream_t st) {
-    constexpr int R = sizeof(Real) == 8 ? 4 : 5;
+    constexpr int R = sizeof(Real) == 8 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS;
     switch (W) {
         case 0: return launch_pass<Real, R, 0>(state, pa, st);
         case 1: return launch_pass<Real, R, 1>(state, pa, st);
@@ -343,7 +343,7 @@ static int launch_chain_rw(State *s, const Plan *p, int iterations, cudaStream_t
 
 template <typename Real>
 static int launch_chain_w(State *s, const Plan *p, int iterations, cudaStream_t st) {
-    constexpr int R = sizeof(Real) == 8 ? 4 : 5;
+    constexpr int R = sizeof(Real) == 8 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS;
     switch (p->warp_bits) {
         case 0: return launch_chain_rw<Real, R, 0>(s, p, iterations, st);
         case 1: return launch_chain_rw<Real, R, 1>(s, p, iterations, st);

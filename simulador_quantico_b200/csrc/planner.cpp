@@ -746,7 +746,7 @@ int build_plan(const std::vector<Op> &ops, int n, const hgm_plan_opts &opts, Pla
     std::vector<SOp> sops = fuse_ops(ops, opts.fuse);
     plan->n_ops = (int64_t)sops.size();
     // amplitudes per thread: 16 for FP64 (64 data registers), 32 for FP32
-    const int R = opts.precision == HGM_F64 ? 4 : 5;
+    const int R = reg_bits_for(opts.precision);
     plan->reg_bits = R;
     if (n < 5 + R || force_small) {
         if (n > 14) return fail(HGM_ERR_UNSUPPORTED, "the shared-memory path takes at most 14 qubits");
