@@ -20,10 +20,10 @@
 #                               backend replaced at link time by
 #                               libhgm_dropin_{f32,f64}.so (only when those
 #                               exist)
-#   oracle/_ref/libref_gpu_f32.so
-#                               the unmodified FP32 core with the reference's
-#                               own GPU backend (src/core/kernel.cu) compiled
-#                               for sm_100a (one scripted fix, see below)
+#   oracle/_ref/libref_gpu_f32.so, {general,grover,shor}_refgpu_f32.out
+#                               the unmodified FP32 core and CLIs with the
+#                               reference's own GPU backend (src/core/kernel.cu)
+#                               compiled for sm_100a (one scripted fix, see below)
 #
 # Sources are read where they lie under the reference tree, whose root the
 # caller names in REF_ROOT (required; nothing is built without it); the widened copy is written to a scratch folder
@@ -115,6 +115,10 @@ build_variant() {
             -o "$work/obj/kernel.o"
         "${NVCC:-nvcc}" -arch=sm_100a -shared -o "$OUT/libref_gpu_$prec.so" $core "$work/obj/kernel.o" \
             "$work/obj/ref_harness.o" -Xcompiler -fopenmp
+        for cli in general grover shor; do
+            "${NVCC:-nvcc}" -arch=sm_100a -o "$OUT/${cli}_refgpu_$prec.out" "$work/obj/$cli.o" $core \
+                "$work/obj/kernel.o" -Xcompiler -fopenmp
+        done
     fi
 
     # Link-time replacement of the GPU backend (makefile:51-61) by the
