@@ -673,6 +673,59 @@ def gate_layers_hbm(sq, n, prec, peak, peak_kind, cases=("hadamard_layer", "rand
     return out
 
 
+def grover_check(sq, peak, peak_kind, n=GROVER_N, mark=GROVER_MARK):
+    """The 26-qubit FP64 Grover search, short form: iterations/s over 3 timed steps of 64 iterations (after one
+    untimed step), then the full 6433-iteration search with its argmax and probability."""
+    spec, c_init, c_one = grover_parts(sq, n, mark)
+    p_init, p_one = sq.Plan(c_init, n, "f64"), sq.Plan(c_one, n, "f64")
+    st = sq.State(n, "f64").set_basis(0).execute(p_init)
+    st.execute(p_one, GROVER_STEP_ITERS)
+    sq.synchronize()
+    with sq.Timer() as t:
+        for _ in range(3):
+            st.execute(p_one, GROVER_STEP_ITERS)
+    iters_s = 3 * GROVER_STEP_ITERS / (t.ms * 1e-3)
+    passes = p_one.stats()["passes"]
+    gbs = passes * 2 * st.nbytes * iters_s / 1e9
+    total = spec.meta["iterations"]
+    with sq.Timer() as t2:
+        st.set_basis(0).execute(p_init).execute(p_one, total)
+    found, pmax = st.marginal_argmax((1 << n) - 1)
+    st.free()
+    return {"iterations_per_s": round(iters_s, 2), "passes_per_iteration": passes, "GB/s": round(gbs, 1),
+            "frac": round(gbs / peak, 4), "peak_source": peak_kind, "full_search_s": round(t2.ms * 1e-3, 3),
+            "iterations": total, "argmax": int(found), "probability": round(pmax, 12),
+            "ok": bool(found == mark and pmax > 0.99)}
+
+
+def batched_check(sq, peak, peak_kind):
+    """The 512-circuit batch (10-22 qubits, half QFT, half 10-layer random circuits), autotuned, FP32 and FP64:
+    circuits/s over 3 graph replays after one untimed replay."""
+    specs = batched_specs(4242, 512)
+    circuits = [spec.build(sq.Circuit()) for spec in specs]
+    out = {}
+    for prec in ("f32", "f64"):
+        b = sq.Batch(prec, 2)
+        for spec, c in zip(specs, circuits):
+            b.add(c, spec.qubits, spec.init_index)
+        tune = b.autotune()
+        b.run()
+        sq.synchronize()
+        with sq.Timer() as t:
+            for _ in range(3):
+                b.run()
+        b.check()
+        size = b.size()
+        ms = t.ms / 3
+        gbs = size["pass_bytes"] / (ms * 1e-3) / 1e9
+        out[prec] = {"circuits_per_s": round(512 / (ms * 1e-3), 1), "ms_per_run": round(ms, 3),
+                     "GB/s": round(gbs, 1), "frac": round(gbs / peak, 4),
+                     "autotune": {"warp_bits": tune["warp_bits"], "low_bits": tune["low_bits"]}}
+        del b
+    out["peak_source"] = peak_kind
+    return out
+
+
 def ref_run_request(spec, prec, threads, gpu=False):
     """Runs one circuit on the reference's own engine the way its algorithm libraries do
     (src/algorithms/lib_general.cpp:30-36, lib_grover.cpp:30-59): a DGM with its state allocated,
@@ -862,6 +915,8 @@ def workload_served(args, dist, sq):
     if not args.skip_layers:
         line["gate_layers_30q_f64"] = gate_layers_hbm(sq, 30, "f64", peak, peak_kind)
         line["layered_32q_f32"] = gate_layers_hbm(sq, 32, "f32", peak, peak_kind, cases=("random_layers_2",))
+        line["grover_26q_f64"] = grover_check(sq, peak, peak_kind)
+        line["batched_512"] = batched_check(sq, peak, peak_kind)
     line["e2e"] = e2e
     if dist.rank == 0 and not args.skip_cpu:
         line["cpu_baseline"] = cpu_baseline_served(args, steps_reqs[args.warmup])
@@ -1131,7 +1186,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-sweep", action="store_true", help="served: no Poisson rate sweep")
     ap.add_argument("--skip-layers", action="store_true",
-                    help="served: no 30-qubit FP64 / 32-qubit FP32 gate-layer measurements")
+                    help="served: none of the other configurations' short measurements (30-qubit FP64 gate layers, "
+                         "32-qubit FP32 layers, 26-qubit Grover, the 512-circuit batch)")
     ap.add_argument("--qubits", type=int, default=0, help="override the workload's qubit count (profiling runs)")
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")
