@@ -144,6 +144,10 @@ struct DevPhase {
 #ifndef HGM_F64_REG_BITS
 #define HGM_F64_REG_BITS 4
 #endif
+// The settings the planner and the tests cover: FP64 4, FP32 4 or 5 (an FP64
+// tile of 2^3 registers left the planner with layouts it cannot build).
+static_assert(HGM_F64_REG_BITS == 4, "FP64 tiles keep 16 amplitudes a thread");
+static_assert(HGM_F32_REG_BITS == 4 || HGM_F32_REG_BITS == 5, "FP32 tiles keep 16 or 32 amplitudes a thread");
 constexpr int reg_bits_for(int precision) { return precision == HGM_F64 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS; }
 
 constexpr int MAX_TILE_BITS = 16;
