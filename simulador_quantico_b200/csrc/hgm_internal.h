@@ -124,6 +124,17 @@ struct PhaseTerm {
     int8_t pad[sizeof(Real) - 3];
     Real a0, a1, pad2;
 };
+// A linear phase term (cbit == PB_LINEAR): many terms of one category whose
+// turns are weights w_b on index bits b folded into one.  It adds
+// scale * value(ix & mask) turns, where value is the masked index as an
+// integer (w_b = scale * 2^b) or, with cval bit 0 set, bit-reversed
+// (w_b = scale * 2^-b: brev64(ix & mask) * 2^-63), and only where index bit
+// tbit is 1 (tbit < 0: always).  The mask takes the bytes of a0 and a1 (FP32)
+// or of a0 (FP64); the scale takes pad2 (FP32) or a1 (FP64).  In a D
+// category a linear term adds to the registers whose bit is 1 (its a0 is 0).
+// The QFT's controlled phases are such runs: the turns 2^-(t-c+1) of the
+// phases on target t from controls c < t are scale 2^-(t+1) times 2^c.
+constexpr int8_t PB_LINEAR = -2;
 template <typename Real>
 constexpr int pb_terms_per_record() {
     return (int)(sizeof(DevOp<Real>) / sizeof(PhaseTerm<Real>));

@@ -598,44 +598,81 @@ struct PhaseBits<Real, A2, R, R> {
 // amplitude, ix = tile base | the thread bits placed at their index bits
 // (head bytes 16..23).  A category's factor is exp(2 pi i * turns), one
 // sincospi per category instead of a complex multiply per term.
+// The words of one compact term.  A linear term (cbit == PB_LINEAR) keeps its
+// index mask where a0 (and, in FP32, a1) sit and its scale in pad2 (FP32) or
+// a1 (FP64).
 template <typename Real>
 struct TermWords;
 template <>
 struct TermWords<float> {
     uint32_t head;
-    float a0, a1;
+    float a0, a1, scale;
+    uint64_t mask;
     __device__ __forceinline__ TermWords(const unsigned char *p) {
         const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p));
         head = v.x;
         a0 = __uint_as_float(v.y);
         a1 = __uint_as_float(v.z);
+        mask = ((uint64_t)v.z << 32) | v.y;
+        scale = __uint_as_float(v.w);
     }
 };
 template <>
 struct TermWords<double> {
     uint32_t head;
-    double a0, a1;
+    double a0, a1, scale;
+    uint64_t mask;
     __device__ __forceinline__ TermWords(const unsigned char *p) {
         const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p));
         const double2 w = __ldg(reinterpret_cast<const double2 *>(p) + 1);
         head = v.x;
         a0 = __hiloint2double((int)v.w, (int)v.z);
         a1 = w.x;
+        mask = ((uint64_t)v.w << 32) | v.z;
+        scale = w.x;
     }
 };
 
-// Term k of the block whose terms start at rec0; c: its control holds, tv:
-// the value of its target bit (0 for a D term).
+// Turns of a linear term at index ix: scale times the masked index as an
+// integer, or bit-reversed (brev64 * 2^-63: index bit b weighs 2^-b).
 template <typename Real>
-__device__ __forceinline__ TermWords<Real> phase_term(const unsigned char *__restrict__ rec0, int k, uint64_t ix,
-                                                      bool &c, uint32_t &tv) {
+__device__ __forceinline__ Real linear_turns(const TermWords<Real> &t, uint64_t ix, bool rev) {
+    const unsigned long long x = ix & t.mask;
+    const Real v = rev ? (Real)__brevll(x) * (Real)1.0842021724855044e-19 : (Real)x;
+    return t.scale * v;
+}
+
+// Term k of the block whose terms start at rec0, for a category that adds
+// a0 / a1 turns by the value of the term's target: the turns it adds at ix
+// (0 where its control does not hold).
+template <typename Real>
+__device__ __forceinline__ Real term_turns(const unsigned char *__restrict__ rec0, int k, uint64_t ix) {
     constexpr int per = pb_terms_per_record<Real>();
     const TermWords<Real> t(rec0 + (k / per) * sizeof(DevOp<Real>) + (k % per) * sizeof(PhaseTerm<Real>));
     const int cbit = (int)(int8_t)(t.head & 0xffu), cval = (int)((t.head >> 8) & 0xffu);
     const int tbit = (int)(int8_t)((t.head >> 16) & 0xffu);
-    c = cbit < 0 || (int)((ix >> (cbit & 63)) & 1u) == cval;
-    tv = tbit < 0 ? 0u : (uint32_t)((ix >> (tbit & 63)) & 1u);
-    return t;
+    const uint32_t tv = tbit < 0 ? 0u : (uint32_t)((ix >> (tbit & 63)) & 1u);
+    if (cbit == PB_LINEAR) return (tbit < 0 || tv) ? linear_turns<Real>(t, ix, cval & 1) : (Real)0;
+    const bool c = cbit < 0 || (int)((ix >> (cbit & 63)) & 1u) == cval;
+    return c ? (tv ? t.a1 : t.a0) : (Real)0;
+}
+
+// Term k of a D category (a diagonal on the category's register bit): adds
+// its d0 turns to h and its d1 turns to g where its control holds.
+template <typename Real>
+__device__ __forceinline__ void dterm_turns(const unsigned char *__restrict__ rec0, int k, uint64_t ix, Real &h,
+                                            Real &g) {
+    constexpr int per = pb_terms_per_record<Real>();
+    const TermWords<Real> t(rec0 + (k / per) * sizeof(DevOp<Real>) + (k % per) * sizeof(PhaseTerm<Real>));
+    const int cbit = (int)(int8_t)(t.head & 0xffu), cval = (int)((t.head >> 8) & 0xffu);
+    if (cbit == PB_LINEAR) {
+        const int tbit = (int)(int8_t)((t.head >> 16) & 0xffu);
+        if (tbit < 0 || ((ix >> (tbit & 63)) & 1u)) g += linear_turns<Real>(t, ix, cval & 1);
+        return;
+    }
+    const bool c = cbit < 0 || (int)((ix >> (cbit & 63)) & 1u) == cval;
+    h += c ? t.a0 : (Real)0;
+    g += c ? t.a1 : (Real)0;
 }
 
 template <typename Real>
@@ -644,19 +681,10 @@ __device__ __forceinline__ Real turns_sum(const unsigned char *__restrict__ rec0
     int k = 0;
 #pragma unroll 1
     for (; k + 1 < n; k += 2) {
-        bool ca, cb;
-        uint32_t ta, tb;
-        const TermWords<Real> x = phase_term<Real>(rec0, k0 + k, ix, ca, ta);
-        const TermWords<Real> y = phase_term<Real>(rec0, k0 + k + 1, ix, cb, tb);
-        acc += ca ? (ta ? x.a1 : x.a0) : (Real)0;
-        acc2 += cb ? (tb ? y.a1 : y.a0) : (Real)0;
+        acc += term_turns<Real>(rec0, k0 + k, ix);
+        acc2 += term_turns<Real>(rec0, k0 + k + 1, ix);
     }
-    if (k < n) {
-        bool ca;
-        uint32_t ta;
-        const TermWords<Real> x = phase_term<Real>(rec0, k0 + k, ix, ca, ta);
-        acc += ca ? (ta ? x.a1 : x.a0) : (Real)0;
-    }
+    if (k < n) acc += term_turns<Real>(rec0, k0 + k, ix);
     return acc + acc2;
 }
 
@@ -679,13 +707,7 @@ struct PhaseBitsAngles {
             Real h = turns_sum<Real>(rec0, k + ng, nh, ix, carry);
             carry = 0;
 #pragma unroll 1
-            for (int i = 0; i < nd; i++) {
-                bool c;
-                uint32_t tv;
-                const TermWords<Real> t = phase_term<Real>(rec0, k + ng + nh + i, ix, c, tv);
-                h += c ? t.a0 : (Real)0;
-                g += c ? t.a1 : (Real)0;
-            }
+            for (int i = 0; i < nd; i++) dterm_turns<Real>(rec0, k + ng + nh + i, ix, h, g);
             // g belongs to the registers whose label has bit B set
             const bool flip = (xr >> B) & 1u;
             const A2 gf = cis_turns<A2>(g), hf = cis_turns<A2>(h);

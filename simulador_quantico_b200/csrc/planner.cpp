@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 
 #include "hgm_internal.h"
 
@@ -259,6 +260,91 @@ DevOp<Real> encode(const SOp &o, const Roles &ro, const int loc_of[64], uint64_t
     return d;
 }
 
+// A phase-block term before encoding: turns a0 / a1 added by the value 0 / 1
+// of the target (index bit tbit, or the category's register bit when tbit <
+// 0), where index bit cbit has value cval (cbit < 0: always).
+struct RawTerm {
+    int cbit, cval, tbit;
+    double a0, a1;
+};
+
+// Writes the linear term (PB_LINEAR) of `bits` -> weight into t if the
+// weights are scale * 2^b (or scale * 2^-b: `rev`) for one scale.
+template <typename Real>
+bool make_linear(const std::map<int, double> &w, int cond_bit, PhaseTerm<Real> &t) {
+    if (w.size() < 2) return false;
+    for (int rev = 0; rev < 2; rev++) {
+        const auto first = *w.begin();
+        const double scale = rev ? std::ldexp(first.second, first.first) : std::ldexp(first.second, -first.first);
+        bool ok = scale != 0.0;
+        uint64_t mask = 0;
+        for (const auto &kv : w) {
+            const double want = rev ? std::ldexp(scale, -kv.first) : std::ldexp(scale, kv.first);
+            ok = ok && std::abs(kv.second - want) <= 1e-12 * std::abs(want);
+            mask |= uint64_t(1) << kv.first;
+        }
+        if (!ok) continue;
+        memset(&t, 0, sizeof t);
+        t.cbit = PB_LINEAR;
+        t.cval = (int8_t)rev;
+        t.tbit = (int8_t)cond_bit;
+        const Real s = (Real)scale;
+        unsigned char *p = reinterpret_cast<unsigned char *>(&t);
+        memcpy(p + sizeof(Real), &mask, sizeof mask);                         // a0 (and a1 for FP32)
+        memcpy(p + (sizeof(Real) == 4 ? 3 : 2) * sizeof(Real), &s, sizeof s);  // pad2 (FP32) or a1 (FP64)
+        return true;
+    }
+    return false;
+}
+
+// The compact terms of one category (kind 0: F; 1: G or H; 2: D).  Terms
+// that add a1 turns where one more index bit is 1 (a0 = 0) are grouped --
+// D: by nothing (the control bit varies), G/H: by nothing (the target bit
+// varies), F: by target (the control bit varies) -- and a group whose
+// weights form a geometric run becomes one linear term.
+template <typename Real>
+std::vector<PhaseTerm<Real>> compact_terms(const std::vector<RawTerm> &raw, int kind) {
+    std::vector<PhaseTerm<Real>> out;
+    std::map<int, std::map<int, double>> groups;  // condition bit -> (varying bit -> summed turns)
+    std::vector<bool> grouped(raw.size(), false);
+    for (size_t i = 0; i < raw.size(); i++) {
+        const RawTerm &t = raw[i];
+        if (std::abs(t.a0) > 1e-15) continue;
+        int cond = -1, bit = -1;
+        if (kind == 2 && t.cbit >= 0 && t.cval == 1 && t.tbit < 0) bit = t.cbit;
+        else if (kind == 1 && t.cbit < 0 && t.tbit >= 0) bit = t.tbit;
+        else if (kind == 0 && t.cbit >= 0 && t.cval == 1 && t.tbit >= 0) {
+            cond = t.tbit;
+            bit = t.cbit;
+        }
+        if (bit < 0) continue;
+        groups[cond][bit] += t.a1;
+        grouped[i] = true;
+    }
+    std::map<int, bool> folded;
+    for (const auto &g : groups) {
+        PhaseTerm<Real> lt;
+        folded[g.first] = make_linear<Real>(g.second, g.first, lt);
+        if (folded[g.first]) out.push_back(lt);
+    }
+    for (size_t i = 0; i < raw.size(); i++) {
+        const RawTerm &t = raw[i];
+        if (grouped[i]) {
+            const int cond = kind == 0 ? t.tbit : -1;
+            if (folded[cond]) continue;
+        }
+        PhaseTerm<Real> p;
+        memset(&p, 0, sizeof p);
+        p.cbit = (int8_t)t.cbit;
+        p.cval = (int8_t)t.cval;
+        p.tbit = (int8_t)t.tbit;
+        p.a0 = (Real)t.a0;
+        p.a1 = (Real)t.a1;
+        out.push_back(p);
+    }
+    return out;
+}
+
 // Phase block (K_PHASE_BLOCK): diagonal gates with at most one control that
 // can all move to the front of what is left, combined into per-thread
 // factors (kernels.cuh apply_phase_block).  Returns false when fewer than
@@ -319,6 +405,29 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
         for (int idx : c)
             for (int k : {0, 3})
                 angles = angles && std::abs(std::abs(ops[idx].m[k]) - 1.0) < 1e-12;
+    // the compact terms of each category, runs of geometric weights folded
+    // into linear terms
+    std::vector<std::vector<PhaseTerm<Real>>> ct(1 + 3 * R);
+    if (angles) {
+        const double turn = 1.0 / (2.0 * 3.14159265358979323846);
+        for (int k = 0; k < 1 + 3 * R; k++) {
+            std::vector<RawTerm> raw;
+            for (int idx : cat[k]) {
+                const SOp &op = ops[idx];
+                const int c_bit = op.cmask ? __builtin_ctzll(op.cmask) : -1;
+                const bool c_reg = c_bit >= 0 && ((tmask >> c_bit) & 1) && ro.of[loc_of[c_bit]].kind == ROLE_REG;
+                const bool t_reg = ((tmask >> op.target) & 1) && ro.of[loc_of[op.target]].kind == ROLE_REG;
+                RawTerm t;
+                t.cbit = c_reg ? -1 : c_bit;  // G/H: the control is the category's register bit
+                t.cval = c_bit >= 0 ? (int)((op.cval >> c_bit) & 1) : 0;
+                t.tbit = t_reg ? -1 : op.target;
+                t.a0 = std::arg(op.m[0]) * turn;
+                t.a1 = std::arg(op.m[3]) * turn;
+                raw.push_back(t);
+            }
+            ct[k] = compact_terms<Real>(raw, k == 0 ? 0 : (k <= 2 * R ? 1 : 2));
+        }
+    }
     DevOp<Real> head;
     memset(&head, 0, sizeof head);
     head.kind = K_PHASE_BLOCK;
@@ -326,9 +435,10 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
     uint8_t counts[16] = {0};
     int nrec = 0;
     for (int k = 0; k < 1 + 3 * R; k++) {
-        counts[k] = (uint8_t)cat[k].size();
-        nrec += (int)cat[k].size();
-        if (cat[k].empty()) continue;
+        const size_t nk = angles ? ct[k].size() : cat[k].size();
+        counts[k] = (uint8_t)nk;
+        nrec += (int)nk;
+        if (!nk) continue;
         head.cv_reg |= k == 0 ? PB_F_ACTIVE : 1u << ((k - 1) % R);
     }
     const int table_recs = has_table ? (1 << R) / 4 : 0;
@@ -345,22 +455,10 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
     if (!angles) {
         for (int idx : order) out.push_back(encode<Real>(ops[idx], ro, loc_of, tmask));
     } else {
-        const double turn = 1.0 / (2.0 * 3.14159265358979323846);
-        std::vector<PhaseTerm<Real>> terms;
-        for (int idx : order) {
-            const SOp &op = ops[idx];
-            PhaseTerm<Real> t;
-            memset(&t, 0, sizeof t);
-            const int c_bit = op.cmask ? __builtin_ctzll(op.cmask) : -1;
-            const bool c_reg = c_bit >= 0 && ((tmask >> c_bit) & 1) && ro.of[loc_of[c_bit]].kind == ROLE_REG;
-            const bool t_reg = ((tmask >> op.target) & 1) && ro.of[loc_of[op.target]].kind == ROLE_REG;
-            t.cbit = (int8_t)(c_reg ? -1 : c_bit);  // G/H: the control is the category's register bit
-            t.cval = (int8_t)(c_bit >= 0 ? (op.cval >> c_bit) & 1 : 0);
-            t.tbit = (int8_t)(t_reg ? -1 : op.target);
-            t.a0 = (Real)(std::arg(op.m[0]) * turn);
-            t.a1 = (Real)(std::arg(op.m[3]) * turn);
-            terms.push_back(t);
-        }
+        // in the kernel's walk order: F, then per register bit b: G[b], H[b], D[b]
+        std::vector<PhaseTerm<Real>> terms(ct[0]);
+        for (int b = 0; b < R; b++)
+            for (int k : {1 + b, 1 + R + b, 1 + 2 * R + b}) terms.insert(terms.end(), ct[k].begin(), ct[k].end());
         for (int r = 0; r < nrec; r++) {
             DevOp<Real> rec;
             memset(&rec, 0, sizeof rec);

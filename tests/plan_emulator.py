@@ -39,6 +39,7 @@ SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"
 K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK = range(9)
 PB_F_ACTIVE = 1 << 16
 REG_BITS = {"f64": 4, "f32": 5}
+PB_LINEAR = -2  # hgm_internal.h: a linear phase term
 
 
 def export(plan, precision):
@@ -172,8 +173,27 @@ def phase_terms(recs, first, count, real):
     for k in range(count):
         raw = recs[first + k // per].tobytes()[(k % per) * size:(k % per + 1) * size]
         t = np.frombuffer(raw, tdt)[0]
-        out.append((int(t["cbit"]), int(t["cval"]), int(t["tbit"]), float(t["a0"]), float(t["a1"])))
+        if int(t["cbit"]) == PB_LINEAR:
+            # linear term: mask where a0 (and a1 in FP32) sit, scale in pad2 (FP32) or a1 (FP64)
+            rs = size // 4
+            mask = int.from_bytes(raw[rs:rs + 8], "little")
+            scale = float(np.frombuffer(raw[3 * rs:4 * rs] if size == 16 else raw[2 * rs:3 * rs], real)[0])
+            out.append(("linear", int(t["cval"]) & 1, int(t["tbit"]), mask, scale))
+        else:
+            out.append((int(t["cbit"]), int(t["cval"]), int(t["tbit"]), float(t["a0"]), float(t["a1"])))
     return out
+
+
+def linear_value(ix, rev, mask, scale):
+    """A linear term's turns: scale times the masked index, or with rev the
+    masked bits weighted 2^-b."""
+    if not rev:
+        return scale * (ix & mask).astype(np.float64)
+    v = np.zeros(ix.shape)
+    for b in range(64):
+        if (mask >> b) & 1:
+            v += ((ix >> b) & 1) * 2.0 ** (-b)
+    return scale * v
 
 
 def apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real):
@@ -192,6 +212,10 @@ def apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real):
     phase = np.zeros((T, 1 << K))
 
     def contrib(term):
+        if term[0] == "linear":
+            _, rev, tbit, mask, scale = term
+            c = np.ones(ix.shape, bool) if tbit < 0 else (((ix >> tbit) & 1) == 1)
+            return c, linear_value(ix, rev, mask, scale)
         cbit, cval, tbit, a0, a1 = term
         c = np.ones(ix.shape, bool) if cbit < 0 else (((ix >> cbit) & 1) == cval)
         t = np.zeros(ix.shape, np.int64) if tbit < 0 else ((ix >> tbit) & 1)
@@ -207,13 +231,15 @@ def apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real):
         for kind, cnt in (("G", counts[1 + b]), ("H", counts[1 + R + b]), ("D", counts[1 + 2 * R + b])):
             for _ in range(int(cnt)):
                 if (act >> b) & 1:
-                    cbit, cval, tbit, a0, a1 = terms[k]
                     c, a = contrib(terms[k])
                     if kind == "G":
                         phase += np.where(c & (bit == 1), a, 0.0)
                     elif kind == "H":
                         phase += np.where(c & (bit == 0), a, 0.0)
+                    elif terms[k][0] == "linear":  # a D term folded: adds where the register bit is 1
+                        phase += np.where(c & (bit == 1), a, 0.0)
                     else:
+                        cbit, cval, tbit, a0, a1 = terms[k]
                         phase += np.where(c, np.where(bit == 1, a1, a0), 0.0)
                 k += 1
     f = np.exp(2j * np.pi * phase)
