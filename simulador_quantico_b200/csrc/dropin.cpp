@@ -13,7 +13,9 @@
 // precision (one cudaMalloc per process instead of one per call), and the
 // plans of the last few PT lists are kept: a call whose list has the same
 // targets, controls and matrices as a cached one (compared in full, not by
-// hash alone) runs that plan instead of planning the list again.
+// hash alone) runs that plan instead of planning the list again.  With
+// HYBRID_DEBUG set (the reference's switch, kernel.cu:304-313) each call
+// prints its elapsed time split into planning, copies and execution.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -167,18 +169,34 @@ hgm_dropin_amp *GpuExecutionWrapper(hgm_dropin_amp *read_memory, hgm_ref_pt **pt
     }
     if (pts == nullptr) die("null PT list");
 
+    auto ms_since = [](std::chrono::steady_clock::time_point t0) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
+    auto t_phase = std::chrono::steady_clock::now();
     hgm_plan *plan = plan_for(pts, qubits);
+    const double plan_ms = ms_since(t_phase);
     hgm_state *state = state_for(qubits);
     if (!state) die("state allocation");
     const int64_t bytes = (int64_t(1) << qubits) * (int64_t)sizeof(hgm_dropin_amp);
+    t_phase = std::chrono::steady_clock::now();
     if (hgm_state_upload(state, read_memory, bytes)) die("copy to device");
+    const double h2d_ms = ms_since(t_phase);
+    t_phase = std::chrono::steady_clock::now();
     if (hgm_execute(state, plan, iterations, nullptr)) die("execution");
+    if (debug && hgm_synchronize()) die("execution");
+    const double exec_ms = ms_since(t_phase);
+    t_phase = std::chrono::steady_clock::now();
     if (hgm_state_download(state, read_memory, bytes)) die("copy to host");
+    const double d2h_ms = ms_since(t_phase);
     if (hgm_plan_status(plan)) die("execution");  // a chained run that gave up a bounded wait
 
     if (debug) {
-        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
-        fprintf(stderr, "[GPUEXEC]   qubits=%d elapsed_ms=%.3f\n", qubits, ms);
+        int64_t n_ops = 0, n_passes = 0;
+        hgm_plan_stats(plan, &n_ops, &n_passes, nullptr, nullptr);
+        fprintf(stderr,
+                "[GPUEXEC]   qubits=%d elapsed_ms=%.3f plan_ms=%.3f h2d_ms=%.3f exec_ms=%.3f d2h_ms=%.3f ops=%lld "
+                "passes=%lld\n",
+                qubits, ms_since(t_start), plan_ms, h2d_ms, exec_ms, d2h_ms, (long long)n_ops, (long long)n_passes);
     }
     return read_memory;
 }
