@@ -15,6 +15,8 @@ Workloads (synthetic, seeded):
            Hadamard benchmark's shape); metric gate-layers/s
   layered  a 30-qubit, 40-layer random Rz/Ry + CNOT circuit in FP64; metric
            gate-layers/s (one step = the whole circuit)
+  qft      the textbook QFT of a basis state, 28 qubits FP32 by default;
+           metric QFT circuits/s
   grover   Grover search, 26 qubits FP64, marked index 42 (the phase
            oracle + diffusion form, no ancilla); metric Grover iterations/s
            (one step = 64 iterations); the full 6433-iteration search is run
@@ -313,6 +315,39 @@ def cpu_baseline_layered(args, kind="reference"):
             "sample": f"{layers_s} layers at {n_s} qubits FP64 t_PAR_CPU ({dt:.2f} s), scaled x{1 << (30 - n_s)} "
                       f"to 30 qubits"}
 
+
+
+def workload_qft(args, dist, sq):
+    """The textbook QFT of a basis state (the served mix's and the batch's QFT requests), 28 qubits FP32 by
+    default (--qubits, --precision); one step = the circuit."""
+    wl = _workloads()
+    n, prec = args.qubits or 28, args.precision
+    spec = wl.qft(n, 0x5A5A5A5 & ((1 << n) - 1))
+    plan = sq.Plan(spec.build(sq.Circuit()), n, prec)
+    stats = plan.stats()
+    st = sq.State(n, prec).set_basis(spec.init_index)
+
+    def step():
+        st.execute(plan)
+
+    with ClockSampler(dist.local_rank) as clk:
+        ms, launches = run_timed(dist, sq, step, args.steps, args.warmup)
+    ms_step = dist.max(ms / args.steps)
+    S = st.nbytes
+    st.free()
+    peak, peak_kind = hbm_peak()
+    achieved = stats["passes"] * 2 * S / (ms_step * 1e-3) / 1e9
+    line = base_line(args, dist, METRICS["qft"], dist.world / (ms_step * 1e-3), "circuits/s", ms_step, prec,
+                     config_for(args))
+    line["plan"] = {"passes_per_step": stats["passes"], "ops_after_fusion": stats["ops"]}
+    line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                        "kernel": "pass_kernel<%s,%d,%d>" % ({"f64": "double", "f32": "float"}[prec], stats["reg_bits"],
+                                                             stats["warp_bits"]),
+                        "algorithmic_bytes_per_launch": 2 * S}
+    line["gpu_launches"] = launches
+    line["clocks"] = clk.summary()
+    return line
 
 
 # ---------------------------------------------------------------------------
@@ -1000,13 +1035,14 @@ def cpu_baseline_served(args, reqs, budget_s=20.0):
 
 
 WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": workload_grover,
-             "batched": workload_batched, "hadamard": workload_hadamard}
+             "batched": workload_batched, "hadamard": workload_hadamard, "qft": workload_qft}
 
 METRICS = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
            "grover": "Grover iterations/s (26q FP64, marked index 42)",
            "hadamard": "gate-layers/s (H on every qubit, 30q FP64)",
            "batched": "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
-           "served": SERVED_METRIC}
+           "served": SERVED_METRIC,
+           "qft": "QFT circuits/s (textbook QFT of a basis state)"}
 
 
 def config_for(args):
@@ -1037,6 +1073,11 @@ def config_for(args):
         S = 16 << n
         return {"workload": f"hadamard-layer-{n}q-fp64", "qubits": n, "gates_per_layer": n, "state_bytes": S,
                 "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"}
+    if w == "qft":
+        n = args.qubits or 28
+        S = (1 << n) * (16 if args.precision == "f64" else 8)
+        return {"workload": f"qft-{n}q", "qubits": n, "precision": {"f64": "fp64", "f32": "fp32"}[args.precision],
+                "state_bytes": S, "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"}
     if w == "grover":
         n = args.qubits or GROVER_N
         S = 16 << n
@@ -1190,7 +1231,8 @@ def main():
                          "32-qubit FP32 layers, 26-qubit Grover, the 512-circuit batch)")
     ap.add_argument("--qubits", type=int, default=0, help="override the workload's qubit count (profiling runs)")
     ap.add_argument("--layers", type=int, default=0, help="override the layered workload's depth (profiling runs)")
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="layered workload amplitude type")
+    ap.add_argument("--precision", default=None, choices=["f64", "f32"],
+                    help="layered / qft amplitude type (default f64 layered, f32 qft)")
     ap.add_argument("--ref-step-s", type=float, default=5.0,
                     help="reference arm, served/batched: seconds of reference work per step")
     args = ap.parse_args()
@@ -1198,6 +1240,8 @@ def main():
         args.steps = 20 if args.workload == "served" else 5
     if args.warmup is None:
         args.warmup = 5 if args.workload == "served" else 3
+    if args.precision is None:
+        args.precision = "f32" if args.workload == "qft" else "f64"
     dist = Dist()
     try:
         if args.impl == "reference":
