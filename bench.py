@@ -1216,7 +1216,7 @@ def main():
     ap.add_argument("--workload", default="served", choices=sorted(WORKLOADS))
     ap.add_argument("--requests", type=int, default=0, help="requests per served step (default 48)")
     ap.add_argument("--rate", type=float, default=0.0, help="Poisson arrival rate in requests/s (0: all at once)")
-    ap.add_argument("--inflight", type=int, default=16, help="server slots")
+    ap.add_argument("--inflight", type=int, default=32, help="server slots")
     ap.add_argument("--plain-limit", type=float, default=60.0, help="seconds cap for the plain FP64 comparison")
     ap.add_argument("--skip-fidelity", action="store_true")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"])

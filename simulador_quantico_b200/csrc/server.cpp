@@ -499,7 +499,7 @@ extern "C" {
 void hgm_server_default_opts(hgm_server_opts *o, int precision) {
     o->precision = precision;
     o->budget_bytes = (int64_t)150 << 30;
-    o->max_inflight = 16;
+    o->max_inflight = 32;  // one per hardware queue (hgm_init asks for 32)
     o->keep_states = 0;
     o->warp_bits = -1;
 }

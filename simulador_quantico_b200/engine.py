@@ -307,7 +307,7 @@ class Batch:
 class Server:
     """Continuous-batching server (include/hgm_b200.h, serving mode)."""
 
-    def __init__(self, precision="f32", budget_bytes=150 << 30, max_inflight=16, keep_states=False, warp_bits=-1):
+    def __init__(self, precision="f32", budget_bytes=150 << 30, max_inflight=32, keep_states=False, warp_bits=-1):
         init()
         o = _lib.ServerOpts()
         lib.hgm_server_default_opts(C.byref(o), PREC[precision])
