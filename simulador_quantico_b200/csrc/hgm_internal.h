@@ -135,13 +135,6 @@ struct PhaseTerm {
 // The QFT's controlled phases are such runs: the turns 2^-(t-c+1) of the
 // phases on target t from controls c < t are scale 2^-(t+1) times 2^c.
 constexpr int8_t PB_LINEAR = -2;
-// A phase block's 2^R table: the complex factors by register label, packed
-// back to back (re, im in the amplitude type) from the start of the records
-// that follow the terms.
-template <typename Real>
-constexpr int pb_table_records(int R) {
-    return (int)(((size_t(1) << R) * 2 * sizeof(Real) + sizeof(DevOp<Real>) - 1) / sizeof(DevOp<Real>));
-}
 template <typename Real>
 constexpr int pb_terms_per_record() {
     return (int)(sizeof(DevOp<Real>) / sizeof(PhaseTerm<Real>));

@@ -445,94 +445,25 @@ __device__ __forceinline__ void load_matrix_flip(const Real *__restrict__ src, R
     }
 }
 
-// ---- FP32 complex layers on packed register pairs --------------------------
-// Blackwell's packed FP32 instructions (fma.rn.f32x2 and mul.rn.f32x2) do
-// two lanes' work in one issue.  For a complex 2x2 gate the lanes must hold
-// the same component of two amplitudes, so an FP32 layer of complex gates
-// first regroups a thread's registers: after soa_exchange, register 2p holds
-// the real parts of amplitudes 2p and 2p+1 and register 2p+1 their imaginary
-// parts (one swap per register pair; the same swap restores the layout).
-#ifndef HGM_F32_PACKED
-#define HGM_F32_PACKED 1
-#endif
-template <int R>
-__device__ __forceinline__ void soa_exchange(float2 (&a)[1 << R]) {
-#pragma unroll
-    for (int j = 0; j < (1 << R); j += 2) {
-        const float t = a[j].y;
-        a[j].y = a[j + 1].x;
-        a[j + 1].x = t;
-    }
-}
-__device__ __forceinline__ float2 splat(float v) { return make_float2(v, v); }
-
-// Dense complex gate on register bit T >= 1 with the registers regrouped:
-// pack p pairs with pack p | 2^(T-1); the same operations in the same order
-// per lane as ip_dense, so the results are bit-identical to the unpacked form.
-template <int R, int T>
-__device__ __forceinline__ void packed_dense(float2 (&a)[1 << R], const float (&m)[8]) {
-    const float2 m0 = splat(m[0]), m1 = splat(m[1]), m2 = splat(m[2]), m3 = splat(m[3]);
-    const float2 m4 = splat(m[4]), m5 = splat(m[5]), m6 = splat(m[6]), m7 = splat(m[7]);
-    const float2 n1 = splat(-m[1]), n3 = splat(-m[3]), n5 = splat(-m[5]), n7 = splat(-m[7]);
-#pragma unroll
-    for (int p = 0; p < (1 << (R - 1)); p++) {
-        if (p & (1 << (T - 1))) continue;
-        const int q = p | (1 << (T - 1));
-        const float2 xr = a[2 * p], xi = a[2 * p + 1], yr = a[2 * q], yi = a[2 * q + 1];
-        a[2 * p] = __ffma2_rn(n3, yi, __ffma2_rn(m2, yr, __ffma2_rn(n1, xi, __fmul2_rn(m0, xr))));
-        a[2 * p + 1] = __ffma2_rn(m2, yi, __ffma2_rn(m3, yr, __ffma2_rn(m1, xr, __fmul2_rn(m0, xi))));
-        a[2 * q] = __ffma2_rn(n7, yi, __ffma2_rn(m6, yr, __ffma2_rn(n5, xi, __fmul2_rn(m4, xr))));
-        a[2 * q + 1] = __ffma2_rn(m6, yi, __ffma2_rn(m7, yr, __ffma2_rn(m5, xr, __fmul2_rn(m4, xi))));
-    }
-}
-
-// The same on register bit 0, whose two values share a pack: lane 0 is the
-// output for bit value 0 (x), lane 1 for 1 (y).  Each lane sums its four
-// products in the order x-real, x-imaginary, y-real, y-imaginary.
-template <int R>
-__device__ __forceinline__ void packed_dense_bit0(float2 (&a)[1 << R], const float (&m)[8]) {
-    // real part: lane 0 = m0 xr - m1 xi + m2 yr - m3 yi, lane 1 = m4 xr - m5 xi + m6 yr - m7 yi
-    const float2 pr0 = make_float2(m[0], m[6]), pr1 = make_float2(-m[1], -m[7]);
-    const float2 pr2 = make_float2(m[2], m[4]), pr3 = make_float2(-m[3], -m[5]);
-    // imaginary part: lane 0 = m0 xi + m1 xr + m2 yi + m3 yr, lane 1 = m4 xi + m5 xr + m6 yi + m7 yr
-    const float2 pi0 = make_float2(m[0], m[6]), pi1 = make_float2(m[1], m[7]);
-    const float2 pi2 = make_float2(m[2], m[4]), pi3 = make_float2(m[3], m[5]);
-#pragma unroll
-    for (int p = 0; p < (1 << (R - 1)); p++) {
-        const float2 re = a[2 * p], im = a[2 * p + 1];
-        const float2 re_sw = make_float2(re.y, re.x), im_sw = make_float2(im.y, im.x);
-        // lane 0 takes x from (re, im) and y from the swapped pairs; lane 1 the other way round
-        a[2 * p] = __ffma2_rn(pr3, im_sw, __ffma2_rn(pr2, re_sw, __ffma2_rn(pr1, im, __fmul2_rn(pr0, re))));
-        a[2 * p + 1] = __ffma2_rn(pi3, re_sw, __ffma2_rn(pi2, im_sw, __ffma2_rn(pi1, re, __fmul2_rn(pi0, im))));
-    }
-}
-
 // A layer: uncontrolled dense gates on a set of register bits (mask),
 // applied bit 0 first, one straight-line block per active bit (a uniform
 // branch skips inactive bits).  Its matrices follow in popcount(mask) records.
-// PACKED: FP32 complex gates on regrouped registers (packed_dense).
-template <typename Real, typename A2, int R, int T, bool REAL, bool PACKED = false>
+template <typename Real, typename A2, int R, int T, bool REAL>
 struct LayerStep {
     __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats, uint32_t mask,
                                                uint32_t xr) {
         if (mask & (1u << T)) {
             Real m[8];
             load_matrix_flip<Real>(mats->m, m, (xr >> T) & 1u);
-            if constexpr (PACKED) {
-                if constexpr (T == 0) packed_dense_bit0<R>(a, m);
-                else packed_dense<R, T>(a, m);
-            } else if (REAL) {
-                reg_real<Real, A2, R, T, false>(a, m, 0u, 0u);
-            } else {
-                reg_dense<Real, A2, R, T, false>(a, m, 0u, 0u);
-            }
+            if (REAL) reg_real<Real, A2, R, T, false>(a, m, 0u, 0u);
+            else reg_dense<Real, A2, R, T, false>(a, m, 0u, 0u);
             mats++;
         }
-        LayerStep<Real, A2, R, T + 1, REAL, PACKED>::run(a, mats, mask, xr);
+        LayerStep<Real, A2, R, T + 1, REAL>::run(a, mats, mask, xr);
     }
 };
-template <typename Real, typename A2, int R, bool REAL, bool PACKED>
-struct LayerStep<Real, A2, R, R, REAL, PACKED> {
+template <typename Real, typename A2, int R, bool REAL>
+struct LayerStep<Real, A2, R, R, REAL> {
     __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, uint32_t,
                                                uint32_t) {}
 };
@@ -766,79 +697,32 @@ __device__ __forceinline__ A2 cis_turns(Real t) {
     return f;
 }
 
-// Angle-form phase blocks: every active register bit B contributes turns g
-// (registers whose label has bit B set) and h (the others).  The turns are
-// gathered first: base takes the F turns and each active bit's h, and d[B]
-// = g - h, so that a register's phase is base plus d[B] for every active bit
-// B its label has.  The label of register r is r ^ xr: where xr has bit B,
-// the physical registers with bit B clear are the ones with label bit B set,
-// so base takes g instead and d[B] = h - g -- then d[B] always goes to the
-// physical registers with bit B set.  Sweeps: the first active bit's
-// multiplies every register (by cis(base) or cis(base + d)), each further
-// active bit only the half of the registers with its bit set.
-template <typename Real, int R, int B>
-struct BitTurns {
-    __device__ __forceinline__ static void run(const unsigned char *__restrict__ rec0, int k, const uint4 &cnt,
-                                               uint32_t act, uint64_t ix, uint32_t xr, Real (&d)[R], Real &base) {
+template <typename Real, typename A2, int R, int B>
+struct PhaseBitsAngles {
+    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const unsigned char *__restrict__ rec0, int k,
+                                               const uint4 &cnt, uint32_t act, Real &carry, uint64_t ix, uint32_t xr) {
         const int ng = count_byte<1 + B>(cnt), nh = count_byte<1 + R + B>(cnt), nd = count_byte<1 + 2 * R + B>(cnt);
         if (act & (1u << B)) {
-            Real g = turns_sum<Real>(rec0, k, ng, ix, (Real)0);
-            Real h = turns_sum<Real>(rec0, k + ng, nh, ix, (Real)0);
+            Real g = turns_sum<Real>(rec0, k, ng, ix, carry);
+            Real h = turns_sum<Real>(rec0, k + ng, nh, ix, carry);
+            carry = 0;
 #pragma unroll 1
             for (int i = 0; i < nd; i++) dterm_turns<Real>(rec0, k + ng + nh + i, ix, h, g);
+            // g belongs to the registers whose label has bit B set
             const bool flip = (xr >> B) & 1u;
-            base += flip ? g : h;
-            d[B] = flip ? h - g : g - h;
-        }
-        BitTurns<Real, R, B + 1>::run(rec0, k + ng + nh + nd, cnt, act, ix, xr, d, base);
-    }
-};
-template <typename Real, int R>
-struct BitTurns<Real, R, R> {
-    __device__ __forceinline__ static void run(const unsigned char *__restrict__, int, const uint4 &, uint32_t,
-                                               uint64_t, uint32_t, Real (&)[R], Real &) {}
-};
-
-template <typename Real, typename A2, int R, int B>
-struct BitSweeps {
-    __device__ __forceinline__ static void run(A2 (&a)[1 << R], uint32_t act, const Real (&d)[R], Real base,
-                                               bool &first) {
-        if (act & (1u << B)) {
-            if (first) {
-                const A2 f0 = cis_turns<A2>(base), f1 = cis_turns<A2>(base + d[B]);
+            const A2 gf = cis_turns<A2>(g), hf = cis_turns<A2>(h);
+            const A2 g1 = flip ? hf : gf, h1 = flip ? gf : hf;
 #pragma unroll
-                for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], ((r >> B) & 1) ? f1 : f0);
-                first = false;
-            } else {
-                const A2 f1 = cis_turns<A2>(d[B]);
-#pragma unroll
-                for (int r = 0; r < (1 << R); r++)
-                    if ((r >> B) & 1) ip_cmul2(a[r], f1);
-            }
+            for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], ((r >> B) & 1) ? g1 : h1);
         }
-        BitSweeps<Real, A2, R, B + 1>::run(a, act, d, base, first);
+        PhaseBitsAngles<Real, A2, R, B + 1>::run(a, rec0, k + ng + nh + nd, cnt, act, carry, ix, xr);
     }
 };
 template <typename Real, typename A2, int R>
-struct BitSweeps<Real, A2, R, R> {
-    __device__ __forceinline__ static void run(A2 (&)[1 << R], uint32_t, const Real (&)[R], Real, bool &) {}
+struct PhaseBitsAngles<Real, A2, R, R> {
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const unsigned char *__restrict__, int, const uint4 &,
+                                               uint32_t, Real &, uint64_t, uint32_t) {}
 };
-
-// The 2^R table (factors by register label, back to back from `recs`):
-// register r takes the factor of its label r ^ xr; with no relabeling the
-// offsets are constants.
-template <typename Real, typename A2, int R>
-__device__ __forceinline__ void table_sweep(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ recs, uint32_t xr) {
-    const A2 *__restrict__ z = reinterpret_cast<const A2 *>(recs);
-    if (xr == 0) {
-#pragma unroll
-        for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], load_c<Real, A2>(reinterpret_cast<const Real *>(z + r)));
-    } else {
-#pragma unroll
-        for (int r = 0; r < (1 << R); r++)
-            ip_cmul2(a[r], load_c<Real, A2>(reinterpret_cast<const Real *>(z + (r ^ xr))));
-    }
-}
 
 template <typename Real, typename A2, int R>
 __device__ __forceinline__ void apply_phase_block_angles(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op,
@@ -857,19 +741,23 @@ __device__ __forceinline__ void apply_phase_block_angles(A2 (&a)[1 << R], const 
     }
     const unsigned char *rec0 = reinterpret_cast<const unsigned char *>(op + 1);
     const int nf = count_byte<0>(cnt);
-    Real turns = turns_sum<Real>(rec0, 0, nf, ix, (Real)0);
-    Real d[R];
-#pragma unroll
-    for (int b = 0; b < R; b++) d[b] = 0;
-    BitTurns<Real, R, 0>::run(rec0, nf, cnt, act, ix, xr, d, turns);
-    bool first = true;
-    BitSweeps<Real, A2, R, 0>::run(a, act, d, turns, first);
-    if (first && (act & PB_F_ACTIVE)) {
-        const A2 f = cis_turns<A2>(turns);
+    Real carry = turns_sum<Real>(rec0, 0, nf, ix, (Real)0);
+    PhaseBitsAngles<Real, A2, R, 0>::run(a, rec0, nf, cnt, act, carry, ix, xr);
+    if ((act & PB_F_ACTIVE) && !(act & ((1u << R) - 1u))) {
+        const A2 f = cis_turns<A2>(carry);
 #pragma unroll
         for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], f);
     }
-    if (has_table) table_sweep<Real, A2, R>(a, op + 1 + nrec - pb_table_records<Real>(R), xr);
+    if (has_table) {
+        const DevOp<Real> *__restrict__ t = op + 1 + nrec - (1 << R) / 4;
+        const Real *__restrict__ z = t->m;
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) {
+            const uint32_t l = r ^ xr;
+            const A2 f = load_c<Real, A2>(z + (l >> 2) * (sizeof(DevOp<Real>) / sizeof(Real)) + 2 * (l & 3));
+            ip_cmul2(a[r], f);
+        }
+    }
 }
 
 // K_PHASE_BLOCK: the F terms fold into one per-thread factor; each active
@@ -895,7 +783,18 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
 #pragma unroll
         for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], carry);
     }
-    if (has_table) table_sweep<Real, A2, R>(a, op + 1 + nrec - pb_table_records<Real>(R), xr);
+    if (has_table) {
+        // 2^R complex factors by register label, four per record, after the
+        // terms; register r holds label r ^ xr
+        t += nrec - (1 << R) / 4;
+        const Real *__restrict__ z = t->m;
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) {
+            const uint32_t l = r ^ xr;
+            const A2 f = load_c<Real, A2>(z + (l >> 2) * (sizeof(DevOp<Real>) / sizeof(Real)) + 2 * (l & 3));
+            ip_cmul2(a[r], f);
+        }
+    }
     return 1 + nrec;
 }
 
@@ -928,15 +827,7 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
     }
     if (kind == K_LAYER || kind == K_LAYER_REAL) {
         const uint32_t mask = hdr.z;  // active register bits
-        if (kind == K_LAYER) {
-            if constexpr (sizeof(Real) == 4 && HGM_F32_PACKED) {
-                soa_exchange<R>(a);
-                LayerStep<Real, A2, R, 0, false, true>::run(a, op + 1, mask, xr);
-                soa_exchange<R>(a);
-            } else {
-                LayerStep<Real, A2, R, 0, false>::run(a, op + 1, mask, xr);
-            }
-        }
+        if (kind == K_LAYER) LayerStep<Real, A2, R, 0, false>::run(a, op + 1, mask, xr);
         else LayerStep<Real, A2, R, 0, true>::run(a, op + 1, mask, xr);
         return;
     }

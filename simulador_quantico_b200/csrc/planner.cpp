@@ -441,7 +441,7 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
         if (!nk) continue;
         head.cv_reg |= k == 0 ? PB_F_ACTIVE : 1u << ((k - 1) % R);
     }
-    const int table_recs = has_table ? pb_table_records<Real>(R) : 0;
+    const int table_recs = has_table ? (1 << R) / 4 : 0;
     constexpr int per = pb_terms_per_record<Real>();
     if (angles) nrec = (nrec + per - 1) / per;
     head.tpos = nrec + table_recs;
@@ -468,16 +468,14 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
             out.push_back(rec);
         }
     }
-    if (table_recs) {
-        // the factors back to back over the table's records
-        std::vector<DevOp<Real>> recs(table_recs);
-        memset(recs.data(), 0, recs.size() * sizeof(DevOp<Real>));
-        Real *z = reinterpret_cast<Real *>(recs.data());
-        for (size_t r = 0; r < table.size(); r++) {
-            z[2 * r] = (Real)table[r].real();
-            z[2 * r + 1] = (Real)table[r].imag();
+    for (int q = 0; q < table_recs; q++) {
+        DevOp<Real> rec;
+        memset(&rec, 0, sizeof rec);
+        for (int k = 0; k < 4; k++) {
+            rec.m[2 * k] = (Real)table[4 * q + k].real();
+            rec.m[2 * k + 1] = (Real)table[4 * q + k].imag();
         }
-        out.insert(out.end(), recs.begin(), recs.end());
+        out.push_back(rec);
     }
     std::vector<int> keep;
     for (int idx : rest)

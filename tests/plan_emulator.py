@@ -244,19 +244,13 @@ def apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real):
                 k += 1
     f = np.exp(2j * np.pi * phase)
     if has_table:
-        f = f * table_factors(recs, i + 1 + nrec - table_records(recs, R), R, real)[reg][None, :]
+        j = i + 1 + nrec - (1 << R) // 4
+        tab = []
+        for q in range((1 << R) // 4):
+            m = recs[j + q]["m"].astype(np.float64)
+            tab += list(m[0::2] + 1j * m[1::2])
+        f = f * np.asarray(tab)[reg][None, :]
     return tile * f
-
-
-def table_records(recs, R):
-    """Records of a phase block's 2^R table: its complex factors back to back."""
-    return -(-(1 << R) * 2 * (recs.dtype["m"].base.itemsize) // recs.dtype.itemsize)
-
-
-def table_factors(recs, first, R, real):
-    raw = b"".join(recs[first + q].tobytes() for q in range(table_records(recs, R)))
-    z = np.frombuffer(raw, dtype=real)[: 2 << R].astype(np.float64)
-    return z[0::2] + 1j * z[1::2]
 
 
 def apply_phase_block(tile, recs, i, R, base, thr, reg, T, K, real="<f8"):
@@ -289,7 +283,11 @@ def apply_phase_block(tile, recs, i, R, base, thr, reg, T, K, real="<f8"):
                 f = np.where(ok, f * fac, f)
                 j += 1
     if has_table:
-        f = f * table_factors(recs, j, R, real)[reg][None, :]
+        tab = []
+        for q in range((1 << R) // 4):
+            m = recs[j + q]["m"].astype(np.float64)
+            tab += list(m[0::2] + 1j * m[1::2])
+        f = f * np.asarray(tab)[reg][None, :]
     return tile * f
 
 
