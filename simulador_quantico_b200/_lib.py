@@ -37,7 +37,8 @@ class Result(C.Structure):
 
 class PlanOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("warp_bits", C.c_int), ("low_bits", C.c_int), ("fuse", C.c_int),
-                ("window", C.c_int), ("renorm_every", C.c_int), ("chained", C.c_int)]
+                ("window", C.c_int), ("renorm_every", C.c_int), ("chained", C.c_int),
+                ("split_layers", C.c_int), ("reg_bits", C.c_int)]
 
 
 def _load():

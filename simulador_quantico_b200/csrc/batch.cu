@@ -268,6 +268,7 @@ int batch_finalize(Batch *b) {
         o.chained = 0;  // the batch kernel runs the passes itself
         o.warp_bits = b->warp_bits;
         o.low_bits = b->low_bits;
+        o.reg_bits = R;  // the batch kernel's tile (compile-time R)
         j.plan.reset(new Plan());
         // a state smaller than one tile runs whole in one CTA's shared memory
         int rc = build_plan(j.ops, j.n, o, j.plan.get(), j.n < K);

@@ -78,7 +78,13 @@ enum DevKind : int32_t {
                        // bytes, cm_reg bit 0: a 2^R table follows, cv_reg:
                        // active categories), then the term records by
                        // category, then the table
+    K_LAYER_SPLIT = 9, // uncontrolled gates diag(1, q) R diag(1, p), R real,
+                       // on the register bits of the mask (cm_reg): one
+                       // record per bit, lowest bit first, with R row-major
+                       // in m[0..3], p in m[4..5] and q in m[6..7]; cv_reg
+                       // bit b: bit b has a p, bit 8 + b: bit b has a q
 };
+constexpr uint32_t SPLIT_POST_SHIFT = 8;
 
 // Phase-block term categories (kernels.cuh apply_phase_block): F multiplies
 // every register; G[b] the registers whose register bit b is 1, H[b] those
@@ -160,6 +166,19 @@ struct DevPhase {
 static_assert(HGM_F64_REG_BITS == 4, "FP64 tiles keep 16 amplitudes a thread");
 static_assert(HGM_F32_REG_BITS == 4 || HGM_F32_REG_BITS == 5, "FP32 tiles keep 16 or 32 amplitudes a thread");
 constexpr int reg_bits_for(int precision) { return precision == HGM_F64 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS; }
+// Register bits of a plan: `requested` (hgm_plan_opts.reg_bits) when valid
+// for the precision, -1 when not; requested < 0 picks reg_bits_for.  FP32
+// plans may keep 16 amplitudes a thread instead of 32.  That measured faster
+// alone for states of at most 20 qubits (Grover, layered and QFT circuits:
+// 5-16% with 8 warps a CTA), slower from 22 qubits (35-55%), and slower for
+// the serving mix as a whole (303 against 345 circuits/s, with 4 warps a
+// CTA), so it is not the default.
+inline int plan_reg_bits(int precision, int qubits, int requested) {
+    (void)qubits;
+    if (precision == HGM_F64) return (requested < 0 || requested == HGM_F64_REG_BITS) ? HGM_F64_REG_BITS : -1;
+    if (requested == 4 || requested == 5) return requested;
+    return requested < 0 ? HGM_F32_REG_BITS : -1;
+}
 
 constexpr int MAX_TILE_BITS = 16;
 // Runs of consecutive non-tile index bits: at most one more than tile bits.

@@ -151,10 +151,10 @@ static int launch_pass(void *state, const PassArgs &pa, cudaStream_t st) {
     return HGM_OK;
 }
 
-// FP64 tiles hold 16 amplitudes a thread (R = 4), FP32 tiles 32 (R = 5).
-template <typename Real>
+// FP64 tiles hold 16 amplitudes a thread (R = 4), FP32 tiles 32 (R = 5) or,
+// on request, 16 (plan_reg_bits).
+template <typename Real, int R>
 static int launch_pass_w(int W, void *state, const PassArgs &pa, cudaStream_t st) {
-    constexpr int R = sizeof(Real) == 8 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS;
     switch (W) {
         case 0: return launch_pass<Real, R, 0>(state, pa, st);
         case 1: return launch_pass<Real, R, 1>(state, pa, st);
@@ -211,8 +211,9 @@ int launch_plan_steps(State *s, const Plan *p, int iterations, PlanCursor *c, in
             c->scale_slot = c->slot;
             c->slot = (c->slot + 1) % 64;
         }
-        int rc = p->precision == HGM_F64 ? launch_pass_w<double>(p->warp_bits, s->d, pa, st)
-                                         : launch_pass_w<float>(p->warp_bits, s->d, pa, st);
+        int rc = p->precision == HGM_F64 ? launch_pass_w<double, HGM_F64_REG_BITS>(p->warp_bits, s->d, pa, st)
+                 : p->reg_bits == 4      ? launch_pass_w<float, 4>(p->warp_bits, s->d, pa, st)
+                                         : launch_pass_w<float, HGM_F32_REG_BITS>(p->warp_bits, s->d, pa, st);
         if (rc) return rc;
     }
     return check("pass_kernel launch");
@@ -341,9 +342,8 @@ static int launch_chain_rw(State *s, const Plan *p, int iterations, cudaStream_t
     return check("chain_kernel launch");
 }
 
-template <typename Real>
+template <typename Real, int R>
 static int launch_chain_w(State *s, const Plan *p, int iterations, cudaStream_t st) {
-    constexpr int R = sizeof(Real) == 8 ? HGM_F64_REG_BITS : HGM_F32_REG_BITS;
     switch (p->warp_bits) {
         case 0: return launch_chain_rw<Real, R, 0>(s, p, iterations, st);
         case 1: return launch_chain_rw<Real, R, 1>(s, p, iterations, st);
@@ -364,8 +364,9 @@ int launch_plan_chain(State *s, const Plan *p, int iterations, void *stream) {
     if (!chain_eligible(p, iterations)) return fail(HGM_ERR_INVALID, "plan not set up for chained passes");
     cudaStream_t st = pick(stream);
     if (!st) return HGM_ERR_CUDA;
-    return p->precision == HGM_F64 ? launch_chain_w<double>(s, p, iterations, st)
-                                   : launch_chain_w<float>(s, p, iterations, st);
+    if (p->precision == HGM_F64) return launch_chain_w<double, HGM_F64_REG_BITS>(s, p, iterations, st);
+    return p->reg_bits == 4 ? launch_chain_w<float, 4>(s, p, iterations, st)
+                            : launch_chain_w<float, HGM_F32_REG_BITS>(s, p, iterations, st);
 }
 
 // Error word of the last chained run of `p` (device address, for an

@@ -468,6 +468,84 @@ struct LayerStep<Real, A2, R, R, REAL> {
                                                uint32_t) {}
 };
 
+template <typename Real, typename A2>
+__device__ __forceinline__ A2 cmul2(A2 a, A2 b);
+
+// Multiplies the registers whose bit T is 1 by f (a phase diag(1, f)).
+template <typename Real, typename A2, int R, int T>
+__device__ __forceinline__ void reg_half_phase(A2 (&a)[1 << R], A2 f) {
+    const Real nfi = -f.y;
+#pragma unroll
+    for (int r = 0; r < (1 << R); r++)
+        if (r & (1 << T)) ip_cmul(a[r].x, a[r].y, f.x, f.y, nfi);
+}
+
+// A split layer (K_LAYER_SPLIT): on each active register bit T the gate
+// diag(1, q) Rm diag(1, p), Rm real, as a phase on the registers whose bit T
+// is 1, the real gate (2 packed FP32 instructions per amplitude) and another
+// phase: 4-6 instructions per amplitude against the complex matrix's 8.
+// Seen through a swapped label (xr bit T set) the gate is
+//   X diag(1, q) Rm diag(1, p) X = p q diag(1, q*) (X Rm X) diag(1, p*),
+// so the phases stay on the same registers, conjugated, the real matrix is
+// read bit-swapped and p q joins the thread's factor `pend`, which the layer
+// multiplies into all registers at its end.
+template <typename Real, typename A2, int R, int T>
+struct SplitStep {
+    __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats,
+                                               uint32_t mask, uint32_t phases, uint32_t xr, A2 &pend) {
+        if (mask & (1u << T)) {
+            const bool flip = (xr >> T) & 1u;
+            const Real *__restrict__ m = mats->m;
+            if (phases & (1u << T)) {
+                A2 p = load_c<Real, A2>(m + 4);
+                const A2 pf = cmul2<Real>(pend, p);
+                pend.x = flip ? pf.x : pend.x;
+                pend.y = flip ? pf.y : pend.y;
+                p.y = flip ? -p.y : p.y;
+                reg_half_phase<Real, A2, R, T>(a, p);
+            }
+            {
+                const A2 r0 = load_c<Real, A2>(m), r1 = load_c<Real, A2>(m + 2);  // (m00, m01), (m10, m11)
+                Real mm[8];
+                mm[0] = flip ? r1.y : r0.x;
+                mm[2] = flip ? r1.x : r0.y;
+                mm[4] = flip ? r0.y : r1.x;
+                mm[6] = flip ? r0.x : r1.y;
+                reg_real<Real, A2, R, T, false>(a, mm, 0u, 0u);
+            }
+            if (phases & (1u << (SPLIT_POST_SHIFT + T))) {
+                A2 q = load_c<Real, A2>(m + 6);
+                const A2 qf = cmul2<Real>(pend, q);
+                pend.x = flip ? qf.x : pend.x;
+                pend.y = flip ? qf.y : pend.y;
+                q.y = flip ? -q.y : q.y;
+                reg_half_phase<Real, A2, R, T>(a, q);
+            }
+            mats++;
+        }
+        SplitStep<Real, A2, R, T + 1>::run(a, mats, mask, phases, xr, pend);
+    }
+};
+template <typename Real, typename A2, int R>
+struct SplitStep<Real, A2, R, R> {
+    __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, uint32_t, uint32_t,
+                                               uint32_t, A2 &) {}
+};
+
+template <typename Real, typename A2, int R>
+__device__ __forceinline__ void apply_split_layer(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats,
+                                                  uint32_t mask, uint32_t phases, uint32_t xr) {
+    A2 pend;
+    pend.x = 1;
+    pend.y = 0;
+    SplitStep<Real, A2, R, 0>::run(a, mats, mask, phases, xr, pend);
+    // every thread of the warp reaches this point (ops are uniform)
+    if (__any_sync(0xffffffffu, pend.x != (Real)1 || pend.y != (Real)0)) {
+#pragma unroll
+        for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], pend);
+    }
+}
+
 // Phase block: diagonal gates with at most one control, combined per thread
 // into a scalar f, per-register-bit factors g[b] (bit 1) and h[b] (bit 0) and
 // an optional host-built 2^R table (gates whose target and control are both
@@ -802,7 +880,7 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
 // and table, a layer's matrices, or the record alone.
 __device__ __forceinline__ int op_records(const uint4 &hdr) {
     if ((int)hdr.x == K_PHASE_BLOCK) return 1 + (int)hdr.y;
-    if ((int)hdr.x == K_LAYER || (int)hdr.x == K_LAYER_REAL) return 1 + __popc(hdr.z);
+    if ((int)hdr.x == K_LAYER || (int)hdr.x == K_LAYER_REAL || (int)hdr.x == K_LAYER_SPLIT) return 1 + __popc(hdr.z);
     return 1;
 }
 
@@ -823,6 +901,10 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
     if (kind == K_PHASE_BLOCK) {
         if (hdr.z & PB_ANGLES) apply_phase_block_angles<Real, A2, R>(a, op, base, thr, xr);
         else apply_phase_block<Real, A2, R>(a, op, base, thr, xr);
+        return;
+    }
+    if (kind == K_LAYER_SPLIT) {
+        apply_split_layer<Real, A2, R>(a, op + 1, hdr.z, hdr.w, xr);
         return;
     }
     if (kind == K_LAYER || kind == K_LAYER_REAL) {

@@ -484,6 +484,34 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
     return true;
 }
 
+// Writes M = s diag(1, q) Rm diag(1, p) with Rm real and |s| = |p| = |q| = 1
+// (the Z-Y-Z form every unitary has: Rz Ry Rz up to a global phase), with s,
+// p and q in the right half plane (a sign goes into Rm) and p or q exactly 1
+// when within 1e-15 of it.  False when an entry is 0 or M has no such form
+// within 1e-14 of its largest entry.
+bool split_gate(const cplx m[4], double rm[4], cplx &s, cplx &p, cplx &q) {
+    double big = 0.0;
+    for (int k = 0; k < 4; k++) {
+        if (m[k] == 0.0) return false;
+        big = std::max(big, std::abs(m[k]));
+    }
+    auto unit = [](cplx z) { return z / std::abs(z); };
+    auto right = [](cplx z) { return (z.real() < 0.0 || (z.real() == 0.0 && z.imag() < 0.0)) ? -z : z; };
+    s = unit(m[0]);
+    p = right(unit(m[1]) / s);
+    q = right(unit(m[2]) / s);
+    s = right(s);
+    if (std::abs(p - 1.0) <= 1e-15) p = 1.0;
+    if (std::abs(q - 1.0) <= 1e-15) q = 1.0;
+    // m_jk = s q^j p^k rm_jk
+    const cplx f[4] = {s, s * p, s * q, s * q * p};
+    for (int k = 0; k < 4; k++) {
+        rm[k] = (m[k] * std::conj(f[k])).real();
+        if (std::abs(m[k] - f[k] * rm[k]) > 1e-14 * big) return false;
+    }
+    return true;
+}
+
 // Emits a phase's gates as a list schedule.  At each step: a phase block if
 // at least three diagonal gates (at most one control each) can move to the
 // front; else a layer -- the uncontrolled dense gates on distinct register
@@ -491,9 +519,12 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
 // (cm_reg holds the mask of those bits, their matrices follow, lowest
 // register bit first) -- if there are at least two; else a phase block of
 // two; else a layer of one; else the first remaining gate on its own record.
+// With `split`, a layer of complex gates that all have the split form
+// (split_gate) goes out as K_LAYER_SPLIT; their scalars s multiply into
+// `global`.
 template <typename Real>
 void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, const Roles &ro, int R, const int loc_of[64],
-                uint64_t tmask, std::vector<DevOp<Real>> &out) {
+                uint64_t tmask, bool split, cplx &global, std::vector<DevOp<Real>> &out) {
     std::vector<int> keep;
     while (!rest.empty()) {
         if (emit_phase_block<Real>(ops, rest, ro, R, loc_of, tmask, 3, out)) continue;
@@ -537,9 +568,34 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, const Roles 
             head.tpos = found;
             for (int k = 0; k < R; k++)
                 if (slot[k] >= 0) head.cm_reg |= 1u << k;
+            // the split form of every gate of the layer, if all have one
+            double rm[8][4];
+            cplx sc[8], pp[8], qq[8];
+            bool all_split = split && !all_real;
+            for (int k = 0; k < R && all_split; k++)
+                if (slot[k] >= 0) all_split = split_gate(ops[slot[k]].m, rm[k], sc[k], pp[k], qq[k]);
+            if (all_split) {
+                head.kind = K_LAYER_SPLIT;
+                for (int k = 0; k < R; k++) {
+                    if (slot[k] < 0) continue;
+                    if (pp[k] != 1.0) head.cv_reg |= 1u << k;
+                    if (qq[k] != 1.0) head.cv_reg |= 1u << (SPLIT_POST_SHIFT + k);
+                }
+            }
             out.push_back(head);
-            for (int k = 0; k < R; k++)
-                if (slot[k] >= 0) out.push_back(encode<Real>(ops[slot[k]], ro, loc_of, tmask));
+            for (int k = 0; k < R; k++) {
+                if (slot[k] < 0) continue;
+                DevOp<Real> d = encode<Real>(ops[slot[k]], ro, loc_of, tmask);
+                if (all_split) {
+                    for (int j = 0; j < 4; j++) d.m[j] = (Real)rm[k][j];
+                    d.m[4] = (Real)pp[k].real();
+                    d.m[5] = (Real)pp[k].imag();
+                    d.m[6] = (Real)qq[k].real();
+                    d.m[7] = (Real)qq[k].imag();
+                    global *= sc[k];
+                }
+                out.push_back(d);
+            }
             for (int idx : rest) {
                 bool member = false;
                 for (int k = 0; k < R; k++) member = member || slot[k] == idx;
@@ -598,7 +654,7 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
     const uint64_t all_bits = (n >= 64) ? ~uint64_t(0) : ((uint64_t(1) << n) - 1);
     std::vector<DevOp<Real>> dev_ops;
     dev_ops.reserve(ops.size());
-    const LayoutMaker lm{R, W, K, R == 4 ? 3 : 4, L};
+    const LayoutMaker lm{R, W, K, sizeof(Real) == 8 ? 3 : 4, L};
     auto intern = [&](const Lay &lay) {
         for (size_t i = 0; i < plan->layouts.size(); i++)
             if (!memcmp(plan->layouts[i].pos, lay.pos, sizeof lay.pos)) return (int)i;
@@ -606,6 +662,8 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
         return (int)plan->layouts.size() - 1;
     };
 
+    // product of the scalars split layers leave out (emit_phase)
+    cplx global = 1.0;
     OpList list((int)ops.size());
     std::vector<int> pass_ops;
     int pass_index = 0;
@@ -771,7 +829,7 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
             ph.op_begin = (int)dev_ops.size();
             Roles ro(plan->layouts[lay], R, W);
             for (int t = 0; t < 5 + W; t++) ro.thr_gbit[t] = pa.tb[plan->layouts[lay].pos[t]];
-            emit_phase<Real>(ops, taken, ro, R, loc_of, tmask, dev_ops);
+            emit_phase<Real>(ops, taken, ro, R, loc_of, tmask, o.split_layers != 0, global, dev_ops);
             ph.op_end = (int)dev_ops.size();
             ph.xwarp = 0;
             if (cur >= 0 && cur != lay) {
@@ -812,6 +870,16 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
         plan->passes.push_back(pa);
         pass_index++;
     }
+    if (global != 1.0) {
+        // the split layers' scalars, once at the end: diag(g, g) on register bit 0
+        DevOp<Real> d;
+        memset(&d, 0, sizeof d);
+        d.kind = K_DIAG;
+        d.m[0] = d.m[6] = (Real)global.real();
+        d.m[1] = d.m[7] = (Real)global.imag();
+        dev_ops.push_back(d);
+        plan->phases.back().op_end = (int)dev_ops.size();
+    }
     plan->ops_bytes.resize(dev_ops.size() * sizeof(DevOp<Real>));
     if (!dev_ops.empty()) memcpy(plan->ops_bytes.data(), dev_ops.data(), plan->ops_bytes.size());
     return HGM_OK;
@@ -844,7 +912,9 @@ int build_plan(const std::vector<Op> &ops, int n, const hgm_plan_opts &opts, Pla
     std::vector<SOp> sops = fuse_ops(ops, opts.fuse);
     plan->n_ops = (int64_t)sops.size();
     // amplitudes per thread: 16 for FP64 (64 data registers), 32 for FP32
-    const int R = reg_bits_for(opts.precision);
+    // (or 16 on request: plan_reg_bits)
+    const int R = plan_reg_bits(opts.precision, n, opts.reg_bits);
+    if (R < 0) return fail(HGM_ERR_INVALID, "reg_bits=%d not available for this precision", opts.reg_bits);
     plan->reg_bits = R;
     if (n < 5 + R || force_small) {
         if (n > 14) return fail(HGM_ERR_UNSUPPORTED, "the shared-memory path takes at most 14 qubits");

@@ -131,14 +131,18 @@ class Plan:
         v = [C.c_int64() for _ in range(4)]
         check(lib.hgm_plan_stats(self.h, *[C.byref(x) for x in v]))
         wb, small = C.c_int(), C.c_int()
-        nph, nb = C.c_int64(), C.c_int64()
-        check(lib.hgm_plan_export(self.h, None, None, None, C.byref(nph), None, C.byref(nb), C.byref(wb),
-                                  C.byref(small)))
+        nph, nb, npa = C.c_int64(), C.c_int64(), C.c_int64()
+        passes = C.c_void_p()
+        check(lib.hgm_plan_export(self.h, C.byref(passes), C.byref(npa), None, C.byref(nph), None, C.byref(nb),
+                                  C.byref(wb), C.byref(small)))
         # bytes copied to the device when the plan is created: op records and phase table
         upload = nb.value + 16 * nph.value
+        # register bits from the first pass's tile bits (struct PassArgs: n, k, ...): k = 5 + R + W
+        reg_bits = 4 if self.precision == HGM_F64 else 5
+        if npa.value and passes.value:
+            reg_bits = C.cast(passes, C.POINTER(C.c_int32))[1] - 5 - wb.value
         return dict(ops=v[0].value, passes=v[1].value, phases=v[2].value, transposes=v[3].value,
-                    warp_bits=wb.value, reg_bits=4 if self.precision == HGM_F64 else 5, small=bool(small.value),
-                    upload_bytes=upload)
+                    warp_bits=wb.value, reg_bits=reg_bits, small=bool(small.value), upload_bytes=upload)
 
 
 class State:

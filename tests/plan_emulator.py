@@ -36,7 +36,8 @@ def op_dtype(real):
 SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f8", 8)]),
             "<f4": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f4", 8)])}
 
-K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK = range(9)
+K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK, K_LAYER_SPLIT = range(10)
+SPLIT_POST_SHIFT = 8
 PB_F_ACTIVE = 1 << 16
 REG_BITS = {"f64": 4, "f32": 5}
 PB_LINEAR = -2  # hgm_internal.h: a linear phase term
@@ -300,10 +301,10 @@ def run(plan, precision, state, iterations=1):
             apply_small(state, e["ops"], n)
         return state
     W = e["W"]
-    R = REG_BITS[precision]
     for _ in range(iterations):
         for pa in e["passes"]:
             K = int(pa["k"])
+            R = K - 5 - W  # the plan's register bits (FP32: 4 or 5)
             lb = getattr(getattr(plan, "opts", None), "low_bits", -1)
             if lb < 0:
                 lb = 3 if precision == "f64" else 4
@@ -342,7 +343,7 @@ def run(plan, precision, state, iterations=1):
                                                  "<f8" if precision == "f64" else "<f4")
                         i += 1 + int(o["tpos"])
                         continue
-                    if int(o["kind"]) in (K_LAYER, K_LAYER_REAL):
+                    if int(o["kind"]) in (K_LAYER, K_LAYER_REAL, K_LAYER_SPLIT):
                         # uncontrolled dense gates on the register bits of the mask, lowest first
                         mask = int(o["cm_reg"])
                         k = 0
@@ -350,7 +351,14 @@ def run(plan, precision, state, iterations=1):
                             if not (mask >> t) & 1:
                                 continue
                             mm = recs[i + 1 + k]["m"].astype(np.float64)
-                            mm = mm[0::2] + 1j * mm[1::2]
+                            if int(o["kind"]) == K_LAYER_SPLIT:
+                                # diag(1, q) Rm diag(1, p): Rm real in m[0..3], p in m[4..5], q in m[6..7]
+                                flags = int(o["cv_reg"])
+                                p = mm[4] + 1j * mm[5] if (flags >> t) & 1 else 1.0
+                                q = mm[6] + 1j * mm[7] if (flags >> (SPLIT_POST_SHIFT + t)) & 1 else 1.0
+                                mm = np.array([mm[0], mm[1] * p, mm[2] * q, mm[3] * q * p], dtype=np.complex128)
+                            else:
+                                mm = mm[0::2] + 1j * mm[1::2]
                             tile = apply_reg_pair(tile, lay, R, W, lane, warp, reg, t, np.ones(T, bool),
                                                   np.ones(1 << K, bool), K_DENSE, mm)
                             k += 1

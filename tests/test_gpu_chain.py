@@ -28,12 +28,13 @@ def run(sq, spec, prec, init, chained, iterations=1, **kw):
     return out, launches, plan.stats()["passes"]
 
 
-@pytest.mark.parametrize("n,prec", [(13, "f64"), (15, "f64"), (21, "f64"), (14, "f32"), (18, "f32"), (22, "f32")])
-def test_chained_equals_per_pass(sq, n, prec):
+@pytest.mark.parametrize("n,prec,reg_bits", [(13, "f64", -1), (15, "f64", -1), (21, "f64", -1), (14, "f32", -1),
+                                              (18, "f32", -1), (22, "f32", -1), (13, "f32", 4), (20, "f32", 4)])
+def test_chained_equals_per_pass(sq, n, prec, reg_bits):
     spec = random_gate_circuit_spec(n, 8 * n, seed=500 + n)
     init = random_state(n, seed=n, dtype=np.complex128 if prec == "f64" else np.complex64)
-    a, la, passes = run(sq, spec, prec, init, 1, renorm_every=0)
-    b, lb, _ = run(sq, spec, prec, init, 0, renorm_every=0)
+    a, la, passes = run(sq, spec, prec, init, 1, renorm_every=0, reg_bits=reg_bits)
+    b, lb, _ = run(sq, spec, prec, init, 0, renorm_every=0, reg_bits=reg_bits)
     assert passes >= 2
     assert la == 1 and lb == passes
     assert np.array_equal(a, b)

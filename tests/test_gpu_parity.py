@@ -106,6 +106,38 @@ def test_random_gates_f32(sq, n, warp_bits):
     assert fidelity_gap(got, want64) < 1e-6
 
 
+@pytest.mark.parametrize("n", [9, 12, 16])
+@pytest.mark.parametrize("warp_bits", [0, 1, 2, 3])
+def test_random_gates_f32_sixteen_registers(sq, n, warp_bits):
+    """FP32 tiles of 16 amplitudes a thread (reg_bits = 4)."""
+    if 9 + warp_bits > n:
+        pytest.skip("tile larger than state")
+    spec = random_gate_circuit_spec(n, 5 * n, seed=n + warp_bits + 40)
+    init = random_state(n, seed=n + 2)
+    got, stats = engine_state(sq, spec, "f32", init=init.astype(np.complex64), warp_bits=warp_bits,
+                              renorm_every=0, reg_bits=4)
+    assert stats["reg_bits"] == 4
+    assert np.abs(got - oracle_state(spec, "f32", init=init.astype(np.complex64))).max() < TOL_F32
+    assert fidelity_gap(got, oracle_state(spec, "f64", init=init)) < 1e-6
+
+
+@pytest.mark.parametrize("n,warp_bits", [(13, 0), (14, 2), (18, 3), (20, 2)])
+def test_split_layers(sq, n, warp_bits):
+    """Layers of Rz.Ry gates as phase, packed real gate, phase, with CNOTs
+    that relabel register bits between them (the relabeled bits take the
+    conjugated phases and the per-thread factor): FP32 and FP64 split plans
+    against the FP64 oracle, and FP32 split against FP32 dense."""
+    spec = wl.random_layered(n, 6, seed=n + 3)
+    want = oracle_state(spec, "f64")
+    got64, _ = engine_state(sq, spec, "f64", warp_bits=warp_bits, split_layers=1)
+    assert np.abs(got64 - want).max() < TOL_F64
+    split, _ = engine_state(sq, spec, "f32", warp_bits=warp_bits, split_layers=1, renorm_every=0)
+    dense, _ = engine_state(sq, spec, "f32", warp_bits=warp_bits, split_layers=0, renorm_every=0)
+    assert fidelity_gap(split, want) < 1e-6
+    assert np.abs(split - want).max() < TOL_F32
+    assert np.abs(split - dense).max() < TOL_F32
+
+
 # ---- benchmark shapes at oracle-checkable sizes --------------------------------
 
 def test_hadamard_benchmark_20q(sq):

@@ -155,3 +155,81 @@ def test_randomized_plans():
         got = emu.run(plan, prec, init)
         want = oracle_state(spec, "f64", init=init)
         assert np.abs(got - want).max() < (1e-11 if prec == "f64" else 5e-5), (case, prec, n, W, lb, spec.name)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("split", [0, 1])
+def test_emulated_split_layers(prec, split):
+    """Layers of complex gates as phase, real gate, phase (K_LAYER_SPLIT) with
+    the gates' scalar factors applied once at the end: the records reproduce
+    the oracle, and split plans hold split layers exactly when asked to."""
+    n = 14
+    tol = 1e-12 if prec == "f64" else 2e-5
+    spec = wl.random_layered(n, 4, seed=31)
+    plan = sq.Plan(spec.build(sq.Circuit()), n, prec, split_layers=split, renorm_every=0)
+    kinds = {int(o["kind"]) for o in emu.export(plan, prec)["ops"]}
+    assert (emu.K_LAYER_SPLIT in kinds) == bool(split)
+    init = random_state(n, seed=4)
+    assert np.abs(emu.run(plan, prec, init) - oracle_state(spec, "f64", init=init)).max() < tol
+
+
+def test_split_layer_gate_forms():
+    """Gates with the split form (Rz Ry, Ry Rz, Rz Ry Rz, a general unitary,
+    a real matrix times a phase) go out as split layers; a complex matrix
+    without it (a column whose entries differ in phase by other than 0 or pi)
+    keeps the dense form; results match the oracle either way."""
+    n = 12
+    rng = np.random.default_rng(5)
+
+    def rz(t):
+        return np.diag([np.exp(-0.5j * t), np.exp(0.5j * t)])
+
+    def ry(t):
+        return np.array([[np.cos(t / 2), -np.sin(t / 2)], [np.sin(t / 2), np.cos(t / 2)]])
+
+    def unitary():
+        q, r = np.linalg.qr(rng.normal(size=(2, 2)) + 1j * rng.normal(size=(2, 2)))
+        return q * (np.diag(r) / np.abs(np.diag(r)))
+
+    forms = [ry(0.4) @ rz(1.1), rz(0.9) @ ry(2.2), rz(0.3) @ ry(1.3) @ rz(2.9), unitary(),
+             np.exp(0.7j) * ry(0.8)]
+    for m in forms:
+        c = sq.Circuit()
+        for q in range(n):
+            c.append_op(q, 0, 0, m)
+        plan = sq.Plan(c, n, "f64", split_layers=1)
+        kinds = [int(o["kind"]) for o in emu.export(plan, "f64")["ops"]]
+        assert emu.K_LAYER_SPLIT in kinds and emu.K_LAYER not in kinds
+        init = random_state(n, seed=6)
+        want = init.reshape([2] * n)
+        for q in range(n):  # index bit q is axis n-1-q
+            want = np.moveaxis(np.tensordot(m, want, axes=([1], [n - 1 - q])), 0, n - 1 - q)
+        assert np.abs(emu.run(plan, "f64", init) - want.reshape(-1)).max() < 1e-12
+    bad = np.array([[1.0, 1.0], [1j, 2.0]]) / 2.0
+    c = sq.Circuit()
+    for q in range(n):
+        c.append_op(q, 0, 0, bad)
+    kinds = [int(o["kind"]) for o in emu.export(sq.Plan(c, n, "f64", split_layers=1), "f64")["ops"]]
+    assert emu.K_LAYER in kinds and emu.K_LAYER_SPLIT not in kinds
+
+
+@pytest.mark.parametrize("n", [9, 10, 12, 14])
+@pytest.mark.parametrize("warp_bits", [0, 1, 2, 3])
+def test_emulated_f32_sixteen_registers(n, warp_bits):
+    """FP32 plans with 16 amplitudes a thread (reg_bits = 4)."""
+    if 9 + warp_bits > n:
+        pytest.skip("tile larger than state")
+    spec = random_gate_circuit_spec(n, 5 * n, seed=77 + n + warp_bits)
+    init = random_state(n, seed=n)
+    plan = sq.Plan(spec.build(sq.Circuit()), n, "f32", reg_bits=4, warp_bits=warp_bits, renorm_every=0)
+    assert plan.stats()["reg_bits"] == 4
+    assert np.abs(emu.run(plan, "f32", init) - oracle_state(spec, "f64", init=init)).max() < 2e-5
+
+
+def test_reg_bits_validated():
+    spec = random_gate_circuit_spec(12, 10, seed=1)
+    for prec, bad in (("f64", 5), ("f64", 3), ("f32", 3), ("f32", 6)):
+        with pytest.raises(Exception):
+            sq.Plan(spec.build(sq.Circuit()), 12, prec, reg_bits=bad)
+    assert sq.Plan(spec.build(sq.Circuit()), 12, "f32").stats()["reg_bits"] == 5
+    assert sq.Plan(spec.build(sq.Circuit()), 12, "f64").stats()["reg_bits"] == 4
