@@ -476,10 +476,11 @@ def grover_parts(sq, n, mark):
 
 def workload_grover(args, dist, sq):
     n, mark = args.qubits or GROVER_N, GROVER_MARK
+    prec = args.precision
     spec, c_init, c_one = grover_parts(sq, n, mark)
     total_iters = spec.meta["iterations"]
-    p_init, p_one = sq.Plan(c_init, n, "f64"), sq.Plan(c_one, n, "f64")
-    st = sq.State(n, "f64").set_basis(0).execute(p_init)
+    p_init, p_one = sq.Plan(c_init, n, prec), sq.Plan(c_one, n, prec)
+    st = sq.State(n, prec).set_basis(0).execute(p_init)
     step_iters = GROVER_STEP_ITERS
 
     def step():
@@ -499,20 +500,22 @@ def workload_grover(args, dist, sq):
     found, pmax = st.marginal_argmax((1 << n) - 1)
     st.free()
     peak, peak_kind = hbm_peak()
-    line = base_line(args, dist, METRICS["grover"], value, "iterations/s", ms_step, "f64", config_for(args))
+    line = base_line(args, dist, METRICS["grover"], value, "iterations/s", ms_step, prec, config_for(args))
     line["plan"] = {"passes_per_iteration": stats["passes"]}
     line["search"] = {"iterations": total_iters, "argmax": int(found), "probability": round(pmax, 12),
                       "ok": bool(found == mark and pmax > 0.99), "timed_iterations_before_check": done}
     line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(achieved / peak, 4),
-                        "traffic": round(TRAFFIC_OVER_ALGO["f64"] * 2 * S / 1e9, 3), "traffic_unit": "GB per launch",
-                        "traffic_source": "ncu capture of the 26-qubit FP64 layered case (same state size)",
+                        "traffic": round(TRAFFIC_OVER_ALGO[prec] * 2 * S / 1e9, 3), "traffic_unit": "GB per launch",
+                        "traffic_source": "ncu capture of the 26-qubit %s layered case (same state size)" % prec.upper(),
                         "peak_source": peak_kind,
-                        "kernel": "pass_kernel<double,%d,%d>" % (stats["reg_bits"], stats["warp_bits"]),
+                        "kernel": "%s<%s,%d,%d>" % ("chain_kernel" if S <= (32 << 20) else "pass_kernel",
+                                                    {"f64": "double", "f32": "float"}[prec], stats["reg_bits"],
+                                                    stats["warp_bits"]),
                         "algorithmic_bytes_per_launch": 2 * S}
     line["gpu_launches"] = launches
     line["clocks"] = clk.summary()
-    line["e2e"] = e2e_grover(dist, sq, c_init, c_one, n, step_iters) if not args.skip_e2e else None
+    line["e2e"] = e2e_grover(dist, sq, c_init, c_one, n, step_iters) if not (args.skip_e2e or prec != "f64") else None
     if dist.rank == 0 and not args.skip_cpu:
         line["cpu_baseline"] = cpu_baseline_grover(args, n, mark)
     return line
@@ -1038,7 +1041,7 @@ WORKLOADS = {"layered": workload_layered, "served": workload_served, "grover": w
              "batched": workload_batched, "hadamard": workload_hadamard, "qft": workload_qft}
 
 METRICS = {"layered": "gate-layers/s (30q random Rz/Ry+CNOT layers)",
-           "grover": "Grover iterations/s (26q FP64, marked index 42)",
+           "grover": "Grover iterations/s (marked index 42; 26q FP64 by default)",
            "hadamard": "gate-layers/s (H on every qubit, 30q FP64)",
            "batched": "batched circuits/s (512 circuits, 10-22 qubits, one persistent kernel)",
            "served": SERVED_METRIC,
@@ -1080,10 +1083,11 @@ def config_for(args):
                 "state_bytes": S, "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"}
     if w == "grover":
         n = args.qubits or GROVER_N
-        S = 16 << n
-        return {"workload": f"grover-{n}q-fp64", "qubits": n, "marked": GROVER_MARK,
-                "iterations_per_step": GROVER_STEP_ITERS, "state_bytes": S,
-                "l2": f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed"}
+        S = (1 << n) * (16 if args.precision == "f64" else 8)
+        l2 = (f"state {S / 2**30:g} GiB > 126 MB L2, no flush needed" if S > (126 << 20) else
+              f"state {S / 2**20:g} MiB stays in L2 (its passes run chained); no flush")
+        return {"workload": f"grover-{n}q-{'fp64' if args.precision == 'f64' else 'fp32'}", "qubits": n,
+                "marked": GROVER_MARK, "iterations_per_step": GROVER_STEP_ITERS, "state_bytes": S, "l2": l2}
     return {"workload": w}
 
 

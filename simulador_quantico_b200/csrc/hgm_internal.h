@@ -101,6 +101,14 @@ constexpr uint32_t PB_F_ACTIVE = 1u << 16;
 // 16..23 hold the index bit of each thread bit (lanes 0..4, warps 5..7).
 constexpr uint32_t PB_HAS_TABLE = 1u;
 constexpr uint32_t PB_ANGLES = 2u;
+// Phase-block head flag (cm_reg, compact terms only): every factor of the
+// block is 1 on the registers whose label bit g is 0 -- its only terms are
+// G[g] and D[g] terms that add nothing where bit g is 0, and its table is 1
+// wherever bit g is 0 -- with g in cm_reg bits PB_GATE_SHIFT.. (the block
+// after the QFT's H on register bit g: controlled phases that all involve g).
+// Such a block multiplies only half the registers, once each.
+constexpr uint32_t PB_GATED = 4u;
+constexpr int PB_GATE_SHIFT = 8;
 
 
 // Target location codes inside a phase: 0..R-1 register bit, 8+q thread bit q

@@ -238,8 +238,16 @@ int64_t plan_launches(const Plan *p, int iterations) {
 // that gives up sets the error word and skips its tile.
 //
 // Scratch (Plan::d_chain): claim counter, done counter, error word, one
-// unused word, then one FP64 norm slot per renormalisation of the sequence.
+// unused word, then CHAIN_NORM_SLOTS FP64 norm slots used in turn, so that a
+// sequence of any length (many iterations of a short FP32 plan) runs chained.
+// Renormalisation k accumulates into slot k % CHAIN_NORM_SLOTS during pass
+// (k + 1) * renorm - 1 and is read during the next pass; tile 0 of the pass
+// before an accumulating pass zeroes its slot before counting itself done, so
+// the zero is seen by every tile of that pass (they wait for the count) and
+// comes after the slot's previous reads (three slots: CHAIN_NORM_SLOTS *
+// renorm > 2 passes apart).
 constexpr unsigned long long CHAIN_WAIT_LIMIT_NS = 2000000000ull;
+constexpr int CHAIN_NORM_SLOTS = 3;
 
 __device__ __forceinline__ unsigned long long chain_now_ns() {
     unsigned long long t;
@@ -294,11 +302,11 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
                 // pass but the last, a rescale on the pass after it
                 if ((g + 1) % renorm == 0 && g + 1 < seq) {
                     flags |= PASS_NORM;
-                    norm_out = norms + ((g + 1) / renorm - 1);
+                    norm_out = norms + ((g + 1) / renorm - 1) % CHAIN_NORM_SLOTS;
                 }
                 if (g > 0 && g % renorm == 0) {
                     flags |= PASS_SCALE;
-                    scale_in = norms + (g / renorm - 1);
+                    scale_in = norms + (g / renorm - 1) % CHAIN_NORM_SLOTS;
                 }
             }
             run_tile<Real, R, W>(state, passes[g % npasses], (uint64_t)(it & ((1ll << tile_bits) - 1)), sm, flags,
@@ -306,6 +314,10 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
         }
         __syncthreads();
         if (threadIdx.x == 0) {
+            const long long g = it >> tile_bits;
+            // the next pass accumulates a norm: zero its slot first
+            if (renorm > 0 && (it & ((1ll << tile_bits) - 1)) == 0 && (g + 2) % renorm == 0 && g + 2 < seq)
+                norms[((g + 2) / renorm - 1) % CHAIN_NORM_SLOTS] = 0.0;
             __threadfence();
             atomicAdd(&ctr[1], 1ull);
         }
@@ -355,7 +367,8 @@ static int launch_chain_w(State *s, const Plan *p, int iterations, cudaStream_t 
 bool chain_eligible(const Plan *p, int iterations) {
     if (p->small || !p->d_chain || p->passes.size() < 2 || iterations < 1) return false;
     const int64_t seq = (int64_t)p->passes.size() * iterations;
-    return p->renorm_every <= 0 || seq / p->renorm_every <= p->chain_slots;
+    (void)seq;
+    return true;
 }
 
 int launch_plan_chain(State *s, const Plan *p, int iterations, void *stream) {
@@ -450,7 +463,7 @@ int upload_plan(Plan *p) {
     const int64_t state_bytes = (int64_t(1) << p->qubits) * (p->precision == HGM_F64 ? 16 : 8);
     if (p->chained && !p->small && p->passes.size() >= 2 && state_bytes <= CHAIN_MAX_BYTES) {
         // chained execution: the pass records (pointers patched) and the scratch
-        p->chain_slots = p->renorm_every > 0 ? (int64_t)p->passes.size() / p->renorm_every + 1 : 0;
+        p->chain_slots = p->renorm_every > 0 ? CHAIN_NORM_SLOTS : 0;
         const size_t sb = (4 + (size_t)p->chain_slots) * sizeof(double);
         const size_t pb = p->passes.size() * sizeof(PassArgs);
         if ((e = plan_alloc(p, 4, &p->d_chain, sb)) != cudaSuccess)

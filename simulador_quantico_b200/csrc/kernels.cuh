@@ -766,6 +766,37 @@ __device__ __forceinline__ void term_diag_product(const DevOp<Real> *__restrict_
     }
 }
 
+// A phase block's 2^R table: complex factors by register label, four per
+// record (the m[] of consecutive records from z), register r holding label
+// r ^ xr.  When no lane of the warp has a relabeled register (xr == 0, as in
+// the QFT's phase passes), the labels are the register numbers and every
+// entry sits at a constant offset: two entries per 16-byte load in FP32 and
+// no address arithmetic, which was most of the integer work of a QFT pass
+// (six instructions per register and table).
+template <typename Real, typename A2, int R>
+__device__ __forceinline__ void apply_table(A2 (&a)[1 << R], const Real *__restrict__ z, uint32_t xr) {
+    constexpr int stride = (int)(sizeof(DevOp<Real>) / sizeof(Real));
+    if (__all_sync(0xffffffffu, xr == 0u)) {
+        if constexpr (sizeof(Real) == 4) {
+#pragma unroll
+            for (int r = 0; r < (1 << R); r += 2) {
+                const float4 f = __ldg(reinterpret_cast<const float4 *>(z + (r >> 2) * stride + 2 * (r & 3)));
+                ip_cmul2(a[r], make_float2(f.x, f.y));
+                ip_cmul2(a[r + 1], make_float2(f.z, f.w));
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], load_c<Real, A2>(z + (r >> 2) * stride + 2 * (r & 3)));
+        }
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < (1 << R); r++) {
+        const uint32_t l = r ^ xr;
+        ip_cmul2(a[r], load_c<Real, A2>(z + (l >> 2) * stride + 2 * (l & 3)));
+    }
+}
+
 // Byte K of the 16 phase-block term counts, kept packed in four words.
 template <int K>
 __device__ __forceinline__ int count_byte(const uint4 &c) {
@@ -937,6 +968,42 @@ struct PhaseBitsAngles<Real, A2, R, R> {
                                                uint32_t, Real &, uint64_t, uint32_t) {}
 };
 
+// Byte k (runtime) of the 16 phase-block term counts.
+__device__ __forceinline__ int count_byte_at(const uint4 &c, int k) {
+    const uint32_t w = k < 4 ? c.x : k < 8 ? c.y : k < 12 ? c.z : c.w;
+    return (int)((w >> (8 * (k & 3))) & 0xffu);
+}
+
+// A gated block's sweep (PB_GATED, no relabeled register in the warp): the
+// registers whose bit B is 1 times c, and times their table entry (read at
+// constant offsets) when the block has a table.
+template <typename Real, typename A2, int R, int B>
+struct GatedSweep {
+    __device__ __forceinline__ static void run(int b, A2 (&a)[1 << R], A2 c, const Real *__restrict__ z) {
+        if (b == B) {
+            constexpr int stride = (int)(sizeof(DevOp<Real>) / sizeof(Real));
+            if (z) {
+#pragma unroll
+                for (int r = 0; r < (1 << R); r++)
+                    if (r & (1 << B)) {
+                        ip_cmul2(a[r], load_c<Real, A2>(z + (r >> 2) * stride + 2 * (r & 3)));
+                        ip_cmul2(a[r], c);
+                    }
+            } else {
+#pragma unroll
+                for (int r = 0; r < (1 << R); r++)
+                    if (r & (1 << B)) ip_cmul2(a[r], c);
+            }
+            return;
+        }
+        GatedSweep<Real, A2, R, B + 1>::run(b, a, c, z);
+    }
+};
+template <typename Real, typename A2, int R>
+struct GatedSweep<Real, A2, R, R> {
+    __device__ __forceinline__ static void run(int, A2 (&)[1 << R], A2, const Real *__restrict__) {}
+};
+
 template <typename Real, typename A2, int R>
 __device__ __forceinline__ void apply_phase_block_angles(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op,
                                                          uint64_t base, uint32_t thr, uint32_t xr) {
@@ -953,6 +1020,17 @@ __device__ __forceinline__ void apply_phase_block_angles(A2 (&a)[1 << R], const 
         ix |= (uint64_t)((thr >> t) & 1u) << g;
     }
     const unsigned char *rec0 = reinterpret_cast<const unsigned char *>(op + 1);
+    if ((hdr.z & PB_GATED) && __all_sync(0xffffffffu, xr == 0u)) {
+        // only G[b] terms, then D[b] terms (the walk order with every other
+        // category empty); one factor for the registers whose bit b is 1
+        const int b = (int)((hdr.z >> PB_GATE_SHIFT) & 7u);
+        const int ng = count_byte_at(cnt, 1 + b), nd = count_byte_at(cnt, 1 + 2 * R + b);
+        Real g = turns_sum<Real>(rec0, 0, ng, ix, (Real)0), h = 0;
+#pragma unroll 1
+        for (int i = 0; i < nd; i++) dterm_turns<Real>(rec0, ng + i, ix, h, g);
+        GatedSweep<Real, A2, R, 0>::run(b, a, cis_turns<A2>(g), has_table ? (op + 1 + nrec - (1 << R) / 4)->m : nullptr);
+        return;
+    }
     const int nf = count_byte<0>(cnt);
     Real carry = turns_sum<Real>(rec0, 0, nf, ix, (Real)0);
     PhaseBitsAngles<Real, A2, R, 0>::run(a, rec0, nf, cnt, act, carry, ix, xr);
@@ -961,16 +1039,7 @@ __device__ __forceinline__ void apply_phase_block_angles(A2 (&a)[1 << R], const 
 #pragma unroll
         for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], f);
     }
-    if (has_table) {
-        const DevOp<Real> *__restrict__ t = op + 1 + nrec - (1 << R) / 4;
-        const Real *__restrict__ z = t->m;
-#pragma unroll
-        for (int r = 0; r < (1 << R); r++) {
-            const uint32_t l = r ^ xr;
-            const A2 f = load_c<Real, A2>(z + (l >> 2) * (sizeof(DevOp<Real>) / sizeof(Real)) + 2 * (l & 3));
-            ip_cmul2(a[r], f);
-        }
-    }
+    if (has_table) apply_table<Real, A2, R>(a, (op + 1 + nrec - (1 << R) / 4)->m, xr);
 }
 
 // K_PHASE_BLOCK: the F terms fold into one per-thread factor; each active
@@ -996,18 +1065,7 @@ __device__ __forceinline__ int apply_phase_block(A2 (&a)[1 << R], const DevOp<Re
 #pragma unroll
         for (int r = 0; r < (1 << R); r++) ip_cmul2(a[r], carry);
     }
-    if (has_table) {
-        // 2^R complex factors by register label, four per record, after the
-        // terms; register r holds label r ^ xr
-        t += nrec - (1 << R) / 4;
-        const Real *__restrict__ z = t->m;
-#pragma unroll
-        for (int r = 0; r < (1 << R); r++) {
-            const uint32_t l = r ^ xr;
-            const A2 f = load_c<Real, A2>(z + (l >> 2) * (sizeof(DevOp<Real>) / sizeof(Real)) + 2 * (l & 3));
-            ip_cmul2(a[r], f);
-        }
-    }
+    if (has_table) apply_table<Real, A2, R>(a, (t + nrec - (1 << R) / 4)->m, xr);
     return 1 + nrec;
 }
 

@@ -428,10 +428,29 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
             ct[k] = compact_terms<Real>(raw, k == 0 ? 0 : (k <= 2 * R ? 1 : 2));
         }
     }
+    // a gate bit: a register bit b such that every factor is 1 where label
+    // bit b is 0 (only G[b] and D[b] terms, D terms adding no d0 turns, and
+    // a table of exact ones wherever bit b is 0)
+    int gate = -1;
+    for (int b = 0; angles && b < R && gate < 0; b++) {
+        bool ok = true;
+        for (int k = 0; k < 1 + 3 * R && ok; k++) {
+            if (ct[k].empty() || k == 1 + b) continue;
+            if (k != 1 + 2 * R + b) {
+                ok = false;
+                continue;
+            }
+            for (const PhaseTerm<Real> &t : ct[k]) ok = ok && (t.cbit == PB_LINEAR || t.a0 == (Real)0);
+        }
+        for (size_t r = 0; has_table && ok && r < table.size(); r++)
+            if (!((r >> b) & 1)) ok = (Real)table[r].real() == (Real)1 && (Real)table[r].imag() == (Real)0;
+        if (ok) gate = b;
+    }
     DevOp<Real> head;
     memset(&head, 0, sizeof head);
     head.kind = K_PHASE_BLOCK;
-    head.cm_reg = (has_table ? PB_HAS_TABLE : 0u) | (angles ? PB_ANGLES : 0u);
+    head.cm_reg = (has_table ? PB_HAS_TABLE : 0u) | (angles ? PB_ANGLES : 0u) |
+                  (gate >= 0 ? PB_GATED | ((uint32_t)gate << PB_GATE_SHIFT) : 0u);
     uint8_t counts[16] = {0};
     int nrec = 0;
     for (int k = 0; k < 1 + 3 * R; k++) {

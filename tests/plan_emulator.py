@@ -41,6 +41,7 @@ SPLIT_POST_SHIFT = 8
 PB_F_ACTIVE = 1 << 16
 REG_BITS = {"f64": 4, "f32": 5}
 PB_LINEAR = -2  # hgm_internal.h: a linear phase term
+PB_GATED, PB_GATE_SHIFT = 4, 8  # hgm_internal.h: a phase block gated by one register bit
 
 
 def export(plan, precision):
@@ -210,6 +211,18 @@ def apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real):
     for t in range(8):
         ix = ix | (((thr >> t) & 1).astype(np.int64) << int(tgb[t]))[None, :]
     terms = phase_terms(recs, i + 1, int(sum(int(c) for c in counts)), real)
+    if int(head["cm_reg"]) & PB_GATED:
+        # the kernel's gated form multiplies only the registers whose label bit
+        # g is 1: every other factor of the block must be exactly 1
+        g = (int(head["cm_reg"]) >> PB_GATE_SHIFT) & 7
+        assert all(int(c) == 0 for k, c in enumerate(counts) if k not in (1 + g, 1 + 2 * R + g)), counts
+        for t in terms[int(counts[1 + g]):]:
+            assert t[0] == "linear" or t[3] == 0.0, t
+        if has_table:
+            j = i + 1 + nrec - (1 << R) // 4
+            tab = np.concatenate([recs[j + q]["m"].astype(np.float64) for q in range((1 << R) // 4)])
+            tab = tab[0::2] + 1j * tab[1::2]
+            assert all(tab[r] == 1.0 for r in range(1 << R) if not (r >> g) & 1)
     phase = np.zeros((T, 1 << K))
 
     def contrib(term):

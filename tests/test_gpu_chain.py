@@ -64,3 +64,22 @@ def test_chained_iterations_and_renorm(sq):
     got4, l4, _ = run(sq, one, "f64", start, 1, iterations=4)
     assert l4 == 1
     assert np.abs(got4 - oracle_state(it_spec, "f64")).max() < TOL_F64
+
+
+def test_chained_many_iterations_fp32_renorm(sq):
+    """A one-iteration FP32 Grover plan run 300 times: 600 passes and 9
+    renormalisations in one launch, through the chained kernel's three norm
+    slots used in turn; the result matches the per-pass launches and the
+    oracle, and stays normalised."""
+    n, w, k = 15, 4321, 300
+    it_spec = wl.grover_search(n, w, iterations=k)
+    (h_steps, _, _), (it_steps, _, _) = it_spec.calls
+    one = wl.CircuitSpec("one", n, 0, it_spec.gates, [(it_steps, 1, True)])
+    start = oracle_state(wl.CircuitSpec("h", n, 0, {}, [([h_steps[0]], 1, True)]), "f64").astype(np.complex64)
+    a, la, passes = run(sq, one, "f32", start, 1, iterations=k)
+    b, lb, _ = run(sq, one, "f32", start, 0, iterations=k)
+    assert la == 1 and lb == passes * k and passes * k > 9 * 64
+    assert np.abs(a - b).max() < 1e-5
+    want = oracle_state(it_spec, "f64")
+    assert np.abs(a - want).max() < 1e-4
+    assert abs(np.vdot(a.astype(np.complex128), a.astype(np.complex128)).real - 1.0) < 1e-4
