@@ -83,8 +83,19 @@ enum DevKind : int32_t {
                        // record per bit, lowest bit first, with R row-major
                        // in m[0..3], p in m[4..5] and q in m[6..7]; cv_reg
                        // bit b: bit b has a p, bit 8 + b: bit b has a q
+    K_XSET = 10,       // X gates on register bits with at most one control, on
+                       // a thread or non-tile bit: tpos entries of 4 bytes
+                       // in m[] (target register bit, control kind
+                       // XSET_CTRL_*, control bit, control value); each flips
+                       // the thread's relabeling mask where its control holds
 };
 constexpr uint32_t SPLIT_POST_SHIFT = 8;
+constexpr int XSET_CTRL_NONE = 0, XSET_CTRL_THREAD = 2, XSET_CTRL_GLOBAL = 3;
+// entries of one K_XSET record: 4 bytes each in m[]
+template <typename Real>
+constexpr int xset_entries() {
+    return (int)(sizeof(Real) * 8 / 4);
+}
 
 // Phase-block term categories (kernels.cuh apply_phase_block): F multiplies
 // every register; G[b] the registers whose register bit b is 1, H[b] those

@@ -1096,6 +1096,28 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
         else apply_phase_block<Real, A2, R>(a, op, base, thr, xr);
         return;
     }
+    if (kind == K_XSET) {
+        // up to 8 (FP32) or 16 (FP64) relabeling X gates, 4 bytes each
+        const uint4 *e = reinterpret_cast<const uint4 *>(op->m);
+        const int n = tpos;
+#pragma unroll
+        for (int q = 0; q < xset_entries<Real>() / 4; q++) {
+            if (4 * q >= n) break;
+            const uint4 w4 = __ldg(e + q);
+            const uint32_t w[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (4 * q + j >= n) break;
+                const uint32_t t = w[j] & 0xffu, ck = (w[j] >> 8) & 0xffu, cb = (w[j] >> 16) & 0xffu,
+                               cv = w[j] >> 24;
+                const uint32_t v = ck == XSET_CTRL_THREAD   ? (thr >> cb) & 1u
+                                   : ck == XSET_CTRL_GLOBAL ? (uint32_t)(base >> cb) & 1u
+                                                            : cv;
+                xr ^= (uint32_t)(v == cv) << t;
+            }
+        }
+        return;
+    }
     if (kind == K_LAYER_SPLIT) {
         apply_split_layer<Real, A2, R>(a, op + 1, hdr.z, hdr.w, xr);
         return;

@@ -503,6 +503,66 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
     return true;
 }
 
+// X gates that only relabel registers (K_XSET): target a register bit of the
+// layout, at most one control, on a thread or non-tile bit.  Takes those that
+// can move to the front of what is left, up to one record's worth; returns
+// whether it emitted a record (one record and no per-gate control checks
+// instead of a record per gate).
+template <typename Real>
+bool emit_xset(const std::vector<SOp> &ops, std::vector<int> &rest, const Roles &ro, const int loc_of[64],
+               uint64_t tmask, std::vector<DevOp<Real>> &out) {
+    constexpr int cap = xset_entries<Real>();
+    std::vector<int> members;
+    uint8_t ent[cap][4];
+    uint64_t bn = 0, bd = 0;
+    for (int idx : rest) {
+        if ((int)members.size() == cap) break;
+        const SOp &op = ops[idx];
+        bool cand = false;
+        const bool is_x = op.mc == MC_ANTI && op.m[1] == 1.0 && op.m[2] == 1.0;
+        if (is_x && __builtin_popcountll(op.cmask) <= 1 && !conflicts(op, bn, bd) && ((tmask >> op.target) & 1)) {
+            const Role tr = ro.of[loc_of[op.target]];
+            if (tr.kind == ROLE_REG) {
+                uint8_t *e = ent[members.size()];
+                e[0] = (uint8_t)tr.idx;
+                e[1] = XSET_CTRL_NONE;
+                e[2] = e[3] = 0;
+                cand = true;
+                if (op.cmask) {
+                    const int c = __builtin_ctzll(op.cmask);
+                    e[3] = (uint8_t)((op.cval >> c) & 1);
+                    if (!((tmask >> c) & 1)) {
+                        e[1] = XSET_CTRL_GLOBAL;
+                        e[2] = (uint8_t)c;
+                    } else if (ro.of[loc_of[c]].kind == ROLE_THREAD) {
+                        e[1] = XSET_CTRL_THREAD;
+                        e[2] = (uint8_t)ro.of[loc_of[c]].idx;
+                    } else {
+                        cand = false;  // a register-bit control swaps amplitudes
+                    }
+                }
+                if (cand) members.push_back(idx);
+            }
+        }
+        if (!cand) {
+            bn |= op.nd();
+            bd |= op.dg();
+        }
+    }
+    if (members.empty()) return false;
+    DevOp<Real> d;
+    memset(&d, 0, sizeof d);
+    d.kind = K_XSET;
+    d.tpos = (int32_t)members.size();
+    memcpy(d.m, ent, members.size() * 4);
+    out.push_back(d);
+    std::vector<int> keep;
+    for (int idx : rest)
+        if (std::find(members.begin(), members.end(), idx) == members.end()) keep.push_back(idx);
+    rest.swap(keep);
+    return true;
+}
+
 // Writes M = s diag(1, q) Rm diag(1, p) with Rm real and |s| = |p| = |q| = 1
 // (the Z-Y-Z form every unitary has: Rz Ry Rz up to a global phase), with s,
 // p and q in the right half plane (a sign goes into Rm) and p or q exactly 1
@@ -537,7 +597,8 @@ bool split_gate(const cplx m[4], double rm[4], cplx &s, cplx &p, cplx &q) {
 // bits of the layout that could all move to the front of what is left
 // (cm_reg holds the mask of those bits, their matrices follow, lowest
 // register bit first) -- if there are at least two; else a phase block of
-// two; else a layer of one; else the first remaining gate on its own record.
+// two; else a layer of one; else the relabeling X gates that can move to the
+// front (K_XSET); else the first remaining gate on its own record.
 // With `split`, a layer of complex gates that all have the split form
 // (split_gate) goes out as K_LAYER_SPLIT; their scalars s multiply into
 // `global`.
@@ -621,6 +682,10 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, const Roles 
                 if (!member) keep.push_back(idx);
             }
         } else if (found != 1 && emit_phase_block<Real>(ops, rest, ro, R, loc_of, tmask, 2, out)) {
+            continue;
+        } else if (emit_xset<Real>(ops, rest, ro, loc_of, tmask, out)) {
+            // relabeling X gates as late as the schedule allows: fewer later
+            // gates see a relabeled bit
             continue;
         } else {
             out.push_back(encode<Real>(ops[rest[0]], ro, loc_of, tmask));

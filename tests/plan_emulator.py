@@ -36,7 +36,8 @@ def op_dtype(real):
 SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f8", 8)]),
             "<f4": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"), ("cval", "<u4"), ("m", "<f4", 8)])}
 
-K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK, K_LAYER_SPLIT = range(10)
+K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK, K_LAYER_SPLIT, K_XSET = range(11)
+XSET_CTRL_NONE, XSET_CTRL_THREAD, XSET_CTRL_GLOBAL = 0, 2, 3
 SPLIT_POST_SHIFT = 8
 PB_F_ACTIVE = 1 << 16
 REG_BITS = {"f64": 4, "f32": 5}
@@ -355,6 +356,21 @@ def run(plan, precision, state, iterations=1):
                         tile = apply_phase_block(tile, recs, i, R, base, thr, reg, T, K,
                                                  "<f8" if precision == "f64" else "<f4")
                         i += 1 + int(o["tpos"])
+                        continue
+                    if int(o["kind"]) == K_XSET:
+                        # relabeling X gates: target register bit, control on a thread or non-tile bit
+                        ent = np.frombuffer(o["m"].tobytes(), np.uint8).reshape(-1, 4)[:int(o["tpos"])]
+                        for t, ck, cb, cv in ent.astype(np.int64):
+                            ok_t = np.ones(T, bool)
+                            ok_j = np.ones(1 << K, bool)
+                            if ck == XSET_CTRL_THREAD:
+                                ok_j = ((thr >> cb) & 1) == cv
+                            elif ck == XSET_CTRL_GLOBAL:
+                                ok_t = ((base >> cb) & 1) == cv
+                            else:
+                                assert ck == XSET_CTRL_NONE and cv == 0
+                            tile = apply_reg_pair(tile, lay, R, W, lane, warp, reg, int(t), ok_t, ok_j, K_SWAP, None)
+                        i += 1
                         continue
                     if int(o["kind"]) in (K_LAYER, K_LAYER_REAL, K_LAYER_SPLIT):
                         # uncontrolled dense gates on the register bits of the mask, lowest first
