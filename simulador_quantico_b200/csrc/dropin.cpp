@@ -146,8 +146,9 @@ hgm_dropin_amp *GpuExecutionWrapper(hgm_dropin_amp *read_memory, hgm_ref_pt **pt
     auto t_start = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lk(g_mu);
 
-    // DGM::validateTuning's GPU rules (src/core/dgm_core.cpp:199-223), kept
-    // at this edge for callers that bypass DGM::execute.
+    // DGM::validateTuning's three GPU rules (src/core/dgm_core.cpp:199-240),
+    // kept at this edge for callers that bypass DGM::execute: the exit status
+    // and the message's first words are the reference's.
     if (2L * block_size * repeat_count != (1L << gpu_region_bits)) {
         printf("Erro de tuning: 2*block_size*repeat_count (%ld) precisa ser igual a 2^gpu_region_bits (%ld)\n",
                2L * block_size * repeat_count, 1L << gpu_region_bits);
@@ -156,6 +157,10 @@ hgm_dropin_amp *GpuExecutionWrapper(hgm_dropin_amp *read_memory, hgm_ref_pt **pt
     if (gpu_region_bits < coalesced_bits) {
         printf("Erro de tuning: gpu_region_bits (%d) precisa ser >= gpu_coalesced_bits (%d)\n", gpu_region_bits,
                coalesced_bits);
+        exit(1);
+    }
+    if (gpu_count > 4) {
+        printf("Erro de tuning: gpu_count (%d) precisa ser <= 4\n", gpu_count);
         exit(1);
     }
     if (gpu_count > 1) {

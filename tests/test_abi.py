@@ -65,3 +65,26 @@ def test_plan_building_is_host_only():
     p = sq.Plan(c, 30, "f64")
     s = p.stats()
     assert s["passes"] >= 3 and s["ops"] <= len(c)
+
+
+@pytest.mark.parametrize("tuning,words", [((4, 8, 1, 32, 2), "2*block_size*repeat_count"),
+                                          ((8, 6, 1, 16, 2), "gpu_region_bits (6)"),
+                                          ((4, 8, 5, 64, 2), "gpu_count (5)")])
+def test_dropin_tuning_rules_exit(tuning, words):
+    """GpuExecutionWrapper refuses the tuning DGM::validateTuning refuses
+    (src/core/dgm_core.cpp:199-240) with the same message start and exit
+    status 1, before any device work (run in a child process, no GPU)."""
+    import subprocess
+    import sys
+
+    code = f"""
+import ctypes as C
+L = C.CDLL({str(LIB / 'libhgm_dropin_f64.so')!r})
+L.GpuExecutionWrapper.argtypes = [C.c_void_p, C.c_void_p] + [C.c_int] * 7
+L.GpuExecutionWrapper.restype = C.c_void_p
+buf = (C.c_double * 2)()
+L.GpuExecutionWrapper(C.addressof(buf), None, 1, *{tuning!r}, 1)
+"""
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1, (r.returncode, r.stdout, r.stderr)
+    assert "Erro de tuning" in r.stdout and words in r.stdout, r.stdout
