@@ -907,7 +907,7 @@ def workload_served(args, dist, sq):
     steps_plans = [[sq.Plan(c, spec.qubits, "f32").upload() for (spec, _), c in zip(reqs, cs)]
                    for reqs, cs in zip(steps_reqs, steps_circuits)]
     upload = [sum(p.stats()["upload_bytes"] for p in plans) for plans in steps_plans]
-    srv = sq.Server("f32", budget_bytes=150 << 30, max_inflight=args.inflight)
+    srv = sq.Server("f32", budget_bytes=150 << 30, max_inflight=args.inflight, order=args.order)
     value, ms, latency, launches, clocks = served_run(args, dist, sq, srv, steps_reqs, steps_plans, True,
                                                       np.random.default_rng(7))
     ms_step = ms / args.steps
@@ -1055,7 +1055,7 @@ def config_for(args):
     if w == "served":
         count = args.requests or 48
         return {"workload": f"served-mix-{count}req", "requests_per_step": count, "rate_hz": args.rate,
-                "max_inflight": args.inflight, "budget_bytes": 150 << 30,
+                "max_inflight": args.inflight, "admission_order": args.order, "budget_bytes": 150 << 30,
                 "precision": "fp32 amplitudes, fp64 gate matrices, norms and argmax",
                 "mix": "60% layered 12-26q d20, 30% QFT 16-28q, 10% Grover 14-20q",
                 "stream": "step s draws its requests from seed 1000 + s",
@@ -1221,6 +1221,8 @@ def main():
     ap.add_argument("--requests", type=int, default=0, help="requests per served step (default 48)")
     ap.add_argument("--rate", type=float, default=0.0, help="Poisson arrival rate in requests/s (0: all at once)")
     ap.add_argument("--inflight", type=int, default=32, help="server slots")
+    ap.add_argument("--order", default="arrival", choices=["arrival", "work_first"],
+                    help="server admission order of queued requests")
     ap.add_argument("--plain-limit", type=float, default=60.0, help="seconds cap for the plain FP64 comparison")
     ap.add_argument("--skip-fidelity", action="store_true")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"])

@@ -275,7 +275,13 @@ typedef struct hgm_server_opts {
     int max_inflight;      /* concurrent requests (streams) */
     int keep_states;       /* 1: finished states stay on the device until hgm_server_release */
     int warp_bits;         /* tile size, -1 = default */
+    int order;             /* HGM_ORDER_ARRIVAL: queued requests are admitted in
+                              arrival order; HGM_ORDER_WORK_FIRST: the queued
+                              request with the most work (state bytes x passes)
+                              that fits the budget goes first */
 } hgm_server_opts;
+#define HGM_ORDER_ARRIVAL 0
+#define HGM_ORDER_WORK_FIRST 1
 
 typedef struct hgm_result {
     int64_t id;

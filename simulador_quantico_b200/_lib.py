@@ -15,6 +15,7 @@ DROPIN = {"f32": LIB_DIR / "libhgm_dropin_f32.so", "f64": LIB_DIR / "libhgm_drop
 
 HGM_OK = 0
 HGM_F64, HGM_F32 = 0, 1
+HGM_ORDER_ARRIVAL, HGM_ORDER_WORK_FIRST = 0, 1
 ERRORS = {1: "invalid", 2: "cuda", 3: "nomem", 4: "unsupported", 5: "timeout", 6: "busy"}
 
 
@@ -26,7 +27,7 @@ class HgmError(RuntimeError):
 
 class ServerOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("budget_bytes", C.c_int64), ("max_inflight", C.c_int),
-                ("keep_states", C.c_int), ("warp_bits", C.c_int)]
+                ("keep_states", C.c_int), ("warp_bits", C.c_int), ("order", C.c_int)]
 
 
 class Result(C.Structure):

@@ -461,16 +461,33 @@ struct Server {
                     progress = true;
                 }
             }
-            // admissions, in arrival order
+            // admissions: in arrival order (the head waits for budget), or the
+            // queued request with the most work that fits
             for (Slot &s : slots) {
                 if (s.req) continue;
                 Request *r = nullptr;
                 {
                     std::lock_guard<std::mutex> lk(mu);
                     if (queue.empty()) break;
-                    if (bytes_in_use + queue.front()->bytes > opts.budget_bytes) break;
-                    r = queue.front();
-                    queue.pop_front();
+                    auto pick = queue.begin();
+                    if (opts.order == HGM_ORDER_WORK_FIRST) {
+                        pick = queue.end();
+                        double best = -1.0;
+                        for (auto it = queue.begin(); it != queue.end(); ++it) {
+                            if (bytes_in_use + (*it)->bytes > opts.budget_bytes) continue;
+                            const Plan *pl = (*it)->plan;
+                            const double w = (double)(*it)->bytes * (pl->small ? 1.0 : (double)pl->passes.size());
+                            if (w > best) {
+                                best = w;
+                                pick = it;
+                            }
+                        }
+                        if (pick == queue.end()) break;
+                    } else if (bytes_in_use + queue.front()->bytes > opts.budget_bytes) {
+                        break;
+                    }
+                    r = *pick;
+                    queue.erase(pick);
                     bytes_in_use += r->bytes;
                     inflight++;
                 }
@@ -502,11 +519,14 @@ void hgm_server_default_opts(hgm_server_opts *o, int precision) {
     o->max_inflight = 32;  // one per hardware queue (hgm_init asks for 32)
     o->keep_states = 0;
     o->warp_bits = -1;
+    o->order = HGM_ORDER_ARRIVAL;
 }
 
 int hgm_server_create(const hgm_server_opts *opts, hgm_server **out) {
     if (!opts || !out) return fail(HGM_ERR_INVALID, "null argument");
     if (opts->max_inflight < 1 || opts->max_inflight > 256) return fail(HGM_ERR_INVALID, "max_inflight outside 1..256");
+    if (opts->order != HGM_ORDER_ARRIVAL && opts->order != HGM_ORDER_WORK_FIRST)
+        return fail(HGM_ERR_INVALID, "unknown admission order %d", opts->order);
     if (!default_stream()) return HGM_ERR_CUDA;
     std::unique_ptr<Server> s(new Server());
     s->opts = *opts;

@@ -311,11 +311,13 @@ class Batch:
 class Server:
     """Continuous-batching server (include/hgm_b200.h, serving mode)."""
 
-    def __init__(self, precision="f32", budget_bytes=150 << 30, max_inflight=32, keep_states=False, warp_bits=-1):
+    def __init__(self, precision="f32", budget_bytes=150 << 30, max_inflight=32, keep_states=False, warp_bits=-1,
+                 order="arrival"):
         init()
         o = _lib.ServerOpts()
         lib.hgm_server_default_opts(C.byref(o), PREC[precision])
         o.budget_bytes, o.max_inflight, o.keep_states, o.warp_bits = budget_bytes, max_inflight, int(keep_states), warp_bits
+        o.order = {"arrival": _lib.HGM_ORDER_ARRIVAL, "work_first": _lib.HGM_ORDER_WORK_FIRST}[order]
         self.precision = PREC[precision]
         self.h = C.c_void_p()
         self.qubits = {}

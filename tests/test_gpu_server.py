@@ -37,9 +37,10 @@ def request_mix(seed, count):
     return reqs
 
 
-def test_served_results_equal_alone(sq):
+@pytest.mark.parametrize("order", ["arrival", "work_first"])
+def test_served_results_equal_alone(sq, order):
     reqs = request_mix(11, 40)
-    srv = sq.Server("f32", budget_bytes=1 << 30, max_inflight=8, keep_states=True)
+    srv = sq.Server("f32", budget_bytes=1 << 30, max_inflight=8, keep_states=True, order=order)
     ids = {}
     for spec, mask in reqs:
         rid = srv.submit(spec.build(sq.Circuit()), spec.qubits, spec.init_index, mask)
@@ -62,9 +63,10 @@ def test_served_results_equal_alone(sq):
     srv.close()
 
 
-def test_admission_respects_budget(sq):
+@pytest.mark.parametrize("order", ["arrival", "work_first"])
+def test_admission_respects_budget(sq, order):
     budget = 4 * (8 << 16)  # four 16-qubit FP32 states
-    srv = sq.Server("f32", budget_bytes=budget, max_inflight=16)
+    srv = sq.Server("f32", budget_bytes=budget, max_inflight=16, order=order)
     n = 16
     for i in range(12):
         spec = wl.random_layered(n, 6, seed=i)
@@ -151,4 +153,22 @@ def test_state_buffers_recycled_within_budget(sq):
         else:
             want = oracle_state(spec, "f64")
             assert r["argmax"] == int(np.argmax(np.abs(want) ** 2))
+    srv.close()
+
+
+def test_work_first_admits_largest(sq):
+    """With one slot, the work-first order admits the queued request with the
+    most work (state bytes x passes) next, not the oldest."""
+    srv = sq.Server("f32", budget_bytes=1 << 30, max_inflight=1, order="work_first")
+    first = wl.random_layered(20, 30, seed=1)  # holds the slot while the rest queue
+    srv.submit_plan(sq.Plan(first.build(sq.Circuit()), 20, "f32").upload(), 0)
+    small = wl.random_layered(12, 2, seed=2)
+    big = wl.random_layered(18, 8, seed=3)
+    plans = [sq.Plan(small.build(sq.Circuit()), 12, "f32").upload(), sq.Plan(big.build(sq.Circuit()), 18, "f32").upload()]
+    rid_small = srv.submit_plan(plans[0], 0)
+    rid_big = srv.submit_plan(plans[1], 0)
+    res = srv.drain(3)
+    assert all(r["status"] == 0 for r in res)
+    queued = {r["id"]: r["queue_s"] for r in res}  # submit -> admitted
+    assert queued[rid_big] < queued[rid_small]
     srv.close()
