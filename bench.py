@@ -811,8 +811,9 @@ def cpu_baseline_batched(args, specs, budget_s=20.0):
         return None
     done, spent, _, _ = ref_stream(specs, "f32", threads, budget_s)
     return {"value": round(done / spent, 6), "unit": "circuits/s", "cores": threads, "kind": "reference",
-            "sample": f"the first {done} of the {len(specs)} circuits in batch order on t_PAR_CPU FP32, each "
-                      f"unscaled, one setFunction + execute per circuit ({spent:.1f} s)"}
+            "sample": (f"the first {done} of the {len(specs)} circuits in batch order" if done <= len(specs) else
+                       f"{done} circuits: the {len(specs)} in batch order, then again from the first") +
+                      f" on t_PAR_CPU FP32, each unscaled, one setFunction + execute per circuit ({spent:.1f} s)"}
 
 
 # ---------------------------------------------------------------------------
