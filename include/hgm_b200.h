@@ -117,7 +117,9 @@ int hgm_plan_create(const hgm_circuit *c, int qubits, const hgm_plan_opts *opts,
 int hgm_plan_create_from_ref_pts(void *const *pts, int pt_precision, int qubits, const hgm_plan_opts *opts,
                                  hgm_plan **out);
 /* Waits for the work queued on the device, then frees the plan: a plan may be
- * freed right after the executions that use it are queued. */
+ * freed right after the executions that use it are queued.  A plan that
+ * requests submitted with hgm_server_submit_plan still use is freed when the
+ * last of them is done. */
 void hgm_plan_free(hgm_plan *p);
 /* Plan statistics: ops after fusion, passes, phases, transposes. */
 int hgm_plan_stats(const hgm_plan *p, int64_t *n_ops, int64_t *n_passes, int64_t *n_phases, int64_t *n_transposes);

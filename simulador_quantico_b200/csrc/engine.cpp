@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 
 #include "hgm_dropin_layout.h"
 #include "hgm_internal.h"
@@ -34,6 +35,32 @@ void ops_from_ref_pts(void *const *pts, std::vector<Op> &out) {
 }
 
 }  // namespace
+
+namespace {
+std::mutex g_lease_mu;
+
+void free_plan_now(Plan *pl) {
+    // launches are asynchronous: the plan's device records may still be in use
+    if (pl->d_ops || pl->d_phases) cudaDeviceSynchronize();
+    delete pl;
+}
+}  // namespace
+
+namespace hgm {
+void plan_lease(const Plan *plan) {
+    std::lock_guard<std::mutex> lk(g_lease_mu);
+    const_cast<Plan *>(plan)->leases++;
+}
+void plan_unlease(const Plan *plan) {
+    Plan *pl = const_cast<Plan *>(plan);
+    bool now = false;
+    {
+        std::lock_guard<std::mutex> lk(g_lease_mu);
+        now = --pl->leases == 0 && pl->free_pending;
+    }
+    if (now) free_plan_now(pl);
+}
+}  // namespace hgm
 
 extern "C" {
 
@@ -116,11 +143,19 @@ int hgm_plan_create_from_ref_pts(void *const *pts, int pt_precision, int qubits,
     return finish_plan(ops, qubits, opts, out);
 }
 
+
 void hgm_plan_free(hgm_plan *p) {
     Plan *pl = reinterpret_cast<Plan *>(p);
-    // launches are asynchronous: the plan's device records may still be in use
-    if (pl && (pl->d_ops || pl->d_phases)) cudaDeviceSynchronize();
-    delete pl;
+    if (!pl) return;
+    {
+        // a plan that queued server requests still use is freed by the last of them
+        std::lock_guard<std::mutex> lk(g_lease_mu);
+        if (pl->leases > 0) {
+            pl->free_pending = true;
+            return;
+        }
+    }
+    free_plan_now(pl);
 }
 
 int hgm_plan_upload(hgm_plan *p) {

@@ -276,6 +276,15 @@ struct Plan {
     void *d_chain_passes = nullptr;
     int64_t chain_slots = 0;
     bool chained = true;              // hgm_plan_opts.chained
+    // The plan runs on the pass kernel's lean build: its phase blocks are all
+    // compact terms, it has no controlled dense, real or anti-diagonal gate on
+    // a register bit and, in FP32, no complex layer (planner, lean_ops).
+    bool lean = false;
+    // Borrowers (requests of a server, hgm_server_submit_plan) hold a lease;
+    // hgm_plan_free on a leased plan only marks it, and the last lease frees
+    // it (plan_lease / plan_unlease, engine.cpp).
+    int leases = 0;
+    bool free_pending = false;
     ~Plan();
 };
 
@@ -293,6 +302,8 @@ int copy_state(void *dst, const void *src, size_t bytes, bool to_device, void *s
 int build_plan(const std::vector<Op> &ops, int qubits, const hgm_plan_opts &opts, Plan *plan,
                bool force_small = false);
 int upload_plan(Plan *plan);
+void plan_lease(const Plan *plan);
+void plan_unlease(const Plan *plan);
 
 // ---- device state ------------------------------------------------------------
 struct State {

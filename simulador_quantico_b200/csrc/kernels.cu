@@ -82,11 +82,11 @@ static inline int check(const char *what) {
 // pass kernels
 // ---------------------------------------------------------------------------
 
-template <typename Real, int R, int W>
+template <typename Real, int R, int W, bool LEAN>
 __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()))
     pass_kernel(typename V2<Real>::T *__restrict__ state, const PassArgs pa) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    run_tile<Real, R, W>(state, pa, blockIdx.x, reinterpret_cast<typename V2<Real>::T *>(smem_raw));
+    run_tile<Real, R, W, LEAN>(state, pa, blockIdx.x, reinterpret_cast<typename V2<Real>::T *>(smem_raw));
 }
 
 template <typename Real>
@@ -125,42 +125,47 @@ __global__ void __launch_bounds__(256) small_kernel(typename V2<Real>::T *__rest
     for (int i = threadIdx.x; i < N; i += blockDim.x) state[i] = sm[i];
 }
 
-template <typename Real, int R, int W>
+template <typename Real, int R, int W, bool LEAN>
 static int setup_pass_kernel() {
     static bool done = false;
     if (done) return HGM_OK;
     const int smem = tile_smem_elems<R, W>() * (int)sizeof(typename V2<Real>::T);
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<Real, R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(pass_kernel<Real, R, W, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess && HGM_SMEM_CARVEOUT >= 0)
-        e = cudaFuncSetAttribute(pass_kernel<Real, R, W>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        e = cudaFuncSetAttribute(pass_kernel<Real, R, W, LEAN>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  HGM_SMEM_CARVEOUT);
     if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
     done = true;
     return HGM_OK;
 }
 
-template <typename Real, int R, int W>
+template <typename Real, int R, int W, bool LEAN>
 static int launch_pass(void *state, const PassArgs &pa, cudaStream_t st) {
     using A2 = typename V2<Real>::T;
-    int rc = setup_pass_kernel<Real, R, W>();
+    int rc = setup_pass_kernel<Real, R, W, LEAN>();
     if (rc) return rc;
     const uint64_t tiles = 1ull << (pa.n - pa.k);
     const int smem = tile_smem_elems<R, W>() * (int)sizeof(A2);
-    pass_kernel<Real, R, W><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<A2 *>(state), pa);
+    pass_kernel<Real, R, W, LEAN><<<(unsigned)tiles, 32 << W, smem, st>>>(reinterpret_cast<A2 *>(state), pa);
     count_launch();
     return HGM_OK;
 }
 
 // FP64 tiles hold 16 amplitudes a thread (R = 4), FP32 tiles 32 (R = 5) or,
 // on request, 16 (plan_reg_bits).
-template <typename Real, int R>
+template <typename Real, int R, bool LEAN>
 static int launch_pass_w(int W, void *state, const PassArgs &pa, cudaStream_t st) {
     switch (W) {
-        case 0: return launch_pass<Real, R, 0>(state, pa, st);
-        case 1: return launch_pass<Real, R, 1>(state, pa, st);
-        case 2: return launch_pass<Real, R, 2>(state, pa, st);
-        default: return launch_pass<Real, R, 3>(state, pa, st);
+        case 0: return launch_pass<Real, R, 0, LEAN>(state, pa, st);
+        case 1: return launch_pass<Real, R, 1, LEAN>(state, pa, st);
+        case 2: return launch_pass<Real, R, 2, LEAN>(state, pa, st);
+        default: return launch_pass<Real, R, 3, LEAN>(state, pa, st);
     }
+}
+template <typename Real, int R>
+static int launch_pass_lw(bool lean, int W, void *state, const PassArgs &pa, cudaStream_t st) {
+    return lean ? launch_pass_w<Real, R, true>(W, state, pa, st) : launch_pass_w<Real, R, false>(W, state, pa, st);
 }
 
 template <typename Real>
@@ -211,9 +216,10 @@ int launch_plan_steps(State *s, const Plan *p, int iterations, PlanCursor *c, in
             c->scale_slot = c->slot;
             c->slot = (c->slot + 1) % 64;
         }
-        int rc = p->precision == HGM_F64 ? launch_pass_w<double, HGM_F64_REG_BITS>(p->warp_bits, s->d, pa, st)
-                 : p->reg_bits == 4      ? launch_pass_w<float, 4>(p->warp_bits, s->d, pa, st)
-                                         : launch_pass_w<float, HGM_F32_REG_BITS>(p->warp_bits, s->d, pa, st);
+        int rc = p->precision == HGM_F64
+                     ? launch_pass_lw<double, HGM_F64_REG_BITS>(p->lean, p->warp_bits, s->d, pa, st)
+                 : p->reg_bits == 4 ? launch_pass_lw<float, 4>(p->lean, p->warp_bits, s->d, pa, st)
+                                    : launch_pass_lw<float, HGM_F32_REG_BITS>(p->lean, p->warp_bits, s->d, pa, st);
         if (rc) return rc;
     }
     return check("pass_kernel launch");
@@ -261,7 +267,7 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
     return v;
 }
 
-template <typename Real, int R, int W>
+template <typename Real, int R, int W, bool LEAN>
 __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()))
     chain_kernel(typename V2<Real>::T *__restrict__ state, const PassArgs *__restrict__ passes, int npasses,
                  int tile_bits, long long total, int renorm, unsigned long long *ctr, double *norms) {
@@ -309,7 +315,7 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
                     scale_in = norms + (g / renorm - 1) % CHAIN_NORM_SLOTS;
                 }
             }
-            run_tile<Real, R, W>(state, passes[g % npasses], (uint64_t)(it & ((1ll << tile_bits) - 1)), sm, flags,
+            run_tile<Real, R, W, LEAN>(state, passes[g % npasses], (uint64_t)(it & ((1ll << tile_bits) - 1)), sm, flags,
                                  norm_out, scale_in);
         }
         __syncthreads();
@@ -324,17 +330,17 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
     }
 }
 
-template <typename Real, int R, int W>
+template <typename Real, int R, int W, bool LEAN>
 static int launch_chain_rw(State *s, const Plan *p, int iterations, cudaStream_t st) {
     using A2 = typename V2<Real>::T;
     static int grid_cap = 0;
     const int smem = tile_smem_elems<R, W>() * (int)sizeof(A2);
     if (!grid_cap) {
-        cudaError_t e = cudaFuncSetAttribute(chain_kernel<Real, R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t e = cudaFuncSetAttribute(chain_kernel<Real, R, W, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         int per_sm = 0, dev = 0, sms = 0;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel<Real, R, W>, 32 << W, smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel<Real, R, W, LEAN>, 32 << W, smem);
         if (e != cudaSuccess || per_sm < 1) return fail(HGM_ERR_CUDA, "chain kernel setup: %s", cudaGetErrorString(e));
         grid_cap = sms * per_sm;
     }
@@ -346,7 +352,7 @@ static int launch_chain_rw(State *s, const Plan *p, int iterations, cudaStream_t
     double *norms = reinterpret_cast<double *>(ctr + 4);
     cudaError_t e = cudaMemsetAsync(p->d_chain, 0, p->d_bytes[4], st);
     if (e != cudaSuccess) return fail(HGM_ERR_CUDA, "chain scratch reset: %s", cudaGetErrorString(e));
-    chain_kernel<Real, R, W><<<grid, 32 << W, smem, st>>>(reinterpret_cast<A2 *>(s->d),
+    chain_kernel<Real, R, W, LEAN><<<grid, 32 << W, smem, st>>>(reinterpret_cast<A2 *>(s->d),
                                                           reinterpret_cast<const PassArgs *>(p->d_chain_passes),
                                                           (int)p->passes.size(), tile_bits, total, p->renorm_every,
                                                           ctr, norms);
@@ -354,14 +360,19 @@ static int launch_chain_rw(State *s, const Plan *p, int iterations, cudaStream_t
     return check("chain_kernel launch");
 }
 
+template <typename Real, int R, bool LEAN>
+static int launch_chain_lw(State *s, const Plan *p, int iterations, cudaStream_t st) {
+    switch (p->warp_bits) {
+        case 0: return launch_chain_rw<Real, R, 0, LEAN>(s, p, iterations, st);
+        case 1: return launch_chain_rw<Real, R, 1, LEAN>(s, p, iterations, st);
+        case 2: return launch_chain_rw<Real, R, 2, LEAN>(s, p, iterations, st);
+        default: return launch_chain_rw<Real, R, 3, LEAN>(s, p, iterations, st);
+    }
+}
 template <typename Real, int R>
 static int launch_chain_w(State *s, const Plan *p, int iterations, cudaStream_t st) {
-    switch (p->warp_bits) {
-        case 0: return launch_chain_rw<Real, R, 0>(s, p, iterations, st);
-        case 1: return launch_chain_rw<Real, R, 1>(s, p, iterations, st);
-        case 2: return launch_chain_rw<Real, R, 2>(s, p, iterations, st);
-        default: return launch_chain_rw<Real, R, 3>(s, p, iterations, st);
-    }
+    return p->lean ? launch_chain_lw<Real, R, true>(s, p, iterations, st)
+                   : launch_chain_lw<Real, R, false>(s, p, iterations, st);
 }
 
 bool chain_eligible(const Plan *p, int iterations) {

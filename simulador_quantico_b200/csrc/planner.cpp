@@ -728,6 +728,40 @@ struct OpList {
     }
 };
 
+// Whether the encoded op records need only the pass kernel's lean build
+// (Plan::lean): phase blocks of compact terms, layers (complex ones in FP64
+// only), relabeling X records, and on register bits only diagonal, phase and
+// X gates.
+template <typename Real>
+bool lean_ops(const std::vector<DevOp<Real>> &d, int R) {
+    for (size_t i = 0; i < d.size();) {
+        const DevOp<Real> &o = d[i];
+        switch (o.kind) {
+            case K_PHASE_BLOCK:
+                if (!(o.cm_reg & PB_ANGLES)) return false;
+                i += 1 + (size_t)o.tpos;
+                break;
+            case K_LAYER:
+                if (sizeof(Real) == 4) return false;
+                i += 1 + (size_t)__builtin_popcount(o.cm_reg);
+                break;
+            case K_LAYER_REAL:
+            case K_LAYER_SPLIT:
+                i += 1 + (size_t)__builtin_popcount(o.cm_reg);
+                break;
+            case K_DENSE:
+            case K_REAL:
+            case K_ANTI:
+                if (o.tpos < R) return false;
+                i++;
+                break;
+            default:
+                i++;
+        }
+    }
+    return true;
+}
+
 template <typename Real>
 int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan *plan) {
     const int W = plan->warp_bits;
@@ -964,6 +998,7 @@ int build_tiled(const std::vector<SOp> &ops, int n, const hgm_plan_opts &o, Plan
         dev_ops.push_back(d);
         plan->phases.back().op_end = (int)dev_ops.size();
     }
+    plan->lean = lean_ops<Real>(dev_ops, R);
     plan->ops_bytes.resize(dev_ops.size() * sizeof(DevOp<Real>));
     if (!dev_ops.empty()) memcpy(plan->ops_bytes.data(), dev_ops.data(), plan->ops_bytes.size());
     return HGM_OK;

@@ -71,6 +71,10 @@ struct Request {
     int status = HGM_OK;
     double norm = 0, pmax = 0;
     int64_t argmax = -1;
+    bool leased = false;  // `plan` is borrowed and leased (hgm_server_submit_plan)
+    ~Request() {
+        if (leased) plan_unlease(plan);
+    }
 };
 
 // Passes are queued on a slot's stream in chunks, at most two chunks ahead
@@ -603,6 +607,8 @@ int hgm_server_submit_plan(hgm_server *ss, const hgm_plan *pp, int64_t init_inde
     const int rc = upload_plan(const_cast<Plan *>(p));
     if (rc) return rc;
     r->plan = p;
+    plan_lease(p);  // a plan freed while the request is queued or running waits for it
+    r->leased = true;
     s->enqueue(r.release(), id);
     return HGM_OK;
 }

@@ -338,8 +338,10 @@ class Server:
         return rid.value
 
     def submit_plan(self, plan: "Plan", init_index: int = 0, result_mask: int = 0) -> int:
-        """Queues an already built (device-resident) plan; the plan must stay
-        alive, and not run elsewhere, until this request's result is polled."""
+        """Queues an already built (device-resident) plan, which must not run
+        elsewhere until this request's result is polled.  The request leases
+        the plan: freeing it (or letting it be collected) before then only
+        marks it, and the server frees it when the request is done."""
         rid = C.c_int64()
         check(lib.hgm_server_submit_plan(self.h, plan.h, init_index, result_mask, C.byref(rid)))
         self.qubits[rid.value] = plan.qubits

@@ -172,3 +172,21 @@ def test_work_first_admits_largest(sq):
     queued = {r["id"]: r["queue_s"] for r in res}  # submit -> admitted
     assert queued[rid_big] < queued[rid_small]
     srv.close()
+
+
+def test_plan_freed_while_queued(sq):
+    """A plan whose Python object is gone right after hgm_server_submit_plan
+    (hgm_plan_free while the request is queued behind a long one) stays valid
+    until the request is done: the request leases it."""
+    import gc
+
+    srv = sq.Server("f32", budget_bytes=1 << 30, max_inflight=1)
+    hold = sq.Plan(wl.random_layered(20, 30, seed=5).build(sq.Circuit()), 20, "f32").upload()
+    srv.submit_plan(hold, 0)
+    spec = wl.qft(14, 1234)
+    rid = srv.submit_plan(sq.Plan(spec.build(sq.Circuit()), 14, "f32").upload(), spec.init_index, (1 << 14) - 1)
+    gc.collect()
+    res = {r["id"]: r for r in srv.drain(2)}
+    assert res[rid]["status"] == 0
+    assert abs(res[rid]["pmax"] - 2.0 ** -14) < 1e-6
+    srv.close()
