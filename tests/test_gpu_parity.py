@@ -138,6 +138,39 @@ def test_split_layers(sq, n, warp_bits):
     assert np.abs(split - dense).max() < TOL_F32
 
 
+def zyz_layered(n, layers, seed):
+    """Layers of Rz.Ry.Rz on every qubit (a phase on both sides of each split
+    gate's real part) and CNOTs on a random matching."""
+    rng = np.random.default_rng(seed)
+    gates, steps = {}, []
+    for layer in range(layers):
+        for tag, fn in (("a", wl.rz), ("b", wl.ry), ("c", wl.rz)):
+            names = []
+            for q in range(n):
+                name = f"{tag}{layer}_{q}"
+                gates[name] = fn(float(rng.uniform(0.0, 2.0 * math.pi)))
+                names.append(name)
+            steps.append(",".join(names))
+        perm = rng.permutation(n)
+        row = ["ID"] * n
+        for g in range(n // 2):
+            row[int(perm[2 * g])] = f"Control{g + 1}(1)"
+            row[int(perm[2 * g + 1])] = f"Target{g + 1}(X)"
+        steps.append(",".join(row))
+    return wl.CircuitSpec("zyz", n, 0, gates, [(steps, 1, True)])
+
+
+@pytest.mark.parametrize("n,warp_bits", [(14, 2), (18, 3)])
+def test_split_layers_post_phase(sq, n, warp_bits):
+    """Split gates with a phase after the real part too (Rz.Ry.Rz), which only
+    the kernels' full build carries: FP32 against the FP64 oracle."""
+    spec = zyz_layered(n, 4, seed=n)
+    want = oracle_state(spec, "f64")
+    got, _ = engine_state(sq, spec, "f32", warp_bits=warp_bits, renorm_every=0)
+    assert np.abs(got - want).max() < TOL_F32
+    assert fidelity_gap(got, want) < 1e-6
+
+
 # ---- benchmark shapes at oracle-checkable sizes --------------------------------
 
 def test_hadamard_benchmark_20q(sq):
