@@ -117,7 +117,8 @@ constexpr uint32_t PB_ANGLES = 2u;
 // G[g] and D[g] terms that add nothing where bit g is 0, and its table is 1
 // wherever bit g is 0 -- with g in cm_reg bits PB_GATE_SHIFT.. (the block
 // after the QFT's H on register bit g: controlled phases that all involve g).
-// Such a block multiplies only half the registers, once each.
+// Such a block multiplies only half the registers, once each, and always has
+// a table (all ones if no term is on register bits only).
 constexpr uint32_t PB_GATED = 4u;
 constexpr int PB_GATE_SHIFT = 8;
 

@@ -978,25 +978,21 @@ __device__ __forceinline__ int count_byte_at(const uint4 &c, int k) {
 }
 
 // A gated block's sweep (PB_GATED, no relabeled register in the warp): the
-// registers whose bit B is 1 times c, and times their table entry (read at
-// constant offsets) when the block has a table.
+// registers whose bit B is 1 times c and their table entry (read at constant
+// offsets).  A gated block always has a table (of ones if nothing else): one
+// body instead of a second one without the table, whose code alone slowed
+// the QFT's passes.
 template <typename Real, typename A2, int R, int B>
 struct GatedSweep {
     __device__ __forceinline__ static void run(int b, A2 (&a)[1 << R], A2 c, const Real *__restrict__ z) {
         if (b == B) {
             constexpr int stride = (int)(sizeof(DevOp<Real>) / sizeof(Real));
-            if (z) {
 #pragma unroll
-                for (int r = 0; r < (1 << R); r++)
-                    if (r & (1 << B)) {
-                        ip_cmul2(a[r], load_c<Real, A2>(z + (r >> 2) * stride + 2 * (r & 3)));
-                        ip_cmul2(a[r], c);
-                    }
-            } else {
-#pragma unroll
-                for (int r = 0; r < (1 << R); r++)
-                    if (r & (1 << B)) ip_cmul2(a[r], c);
-            }
+            for (int r = 0; r < (1 << R); r++)
+                if (r & (1 << B)) {
+                    ip_cmul2(a[r], load_c<Real, A2>(z + (r >> 2) * stride + 2 * (r & 3)));
+                    ip_cmul2(a[r], c);
+                }
             return;
         }
         GatedSweep<Real, A2, R, B + 1>::run(b, a, c, z);
@@ -1031,7 +1027,7 @@ __device__ __forceinline__ void apply_phase_block_angles(A2 (&a)[1 << R], const 
         Real g = turns_sum<Real>(rec0, 0, ng, ix, (Real)0), h = 0;
 #pragma unroll 1
         for (int i = 0; i < nd; i++) dterm_turns<Real>(rec0, ng + i, ix, h, g);
-        GatedSweep<Real, A2, R, 0>::run(b, a, cis_turns<A2>(g), has_table ? (op + 1 + nrec - (1 << R) / 4)->m : nullptr);
+        GatedSweep<Real, A2, R, 0>::run(b, a, cis_turns<A2>(g), (op + 1 + nrec - (1 << R) / 4)->m);
         return;
     }
     const int nf = count_byte<0>(cnt);

@@ -446,6 +446,9 @@ bool emit_phase_block(const std::vector<SOp> &ops, std::vector<int> &rest, const
             if (!((r >> b) & 1)) ok = (Real)table[r].real() == (Real)1 && (Real)table[r].imag() == (Real)0;
         if (ok) gate = b;
     }
+    // a gated block always carries its table (ones where no term reaches), so
+    // that the kernel's gated sweep has one form
+    if (gate >= 0) has_table = true;
     DevOp<Real> head;
     memset(&head, 0, sizeof head);
     head.kind = K_PHASE_BLOCK;

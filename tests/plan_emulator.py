@@ -216,6 +216,7 @@ def apply_phase_block_angles(tile, recs, i, R, base, thr, reg, T, K, real):
         # the kernel's gated form multiplies only the registers whose label bit
         # g is 1: every other factor of the block must be exactly 1
         g = (int(head["cm_reg"]) >> PB_GATE_SHIFT) & 7
+        assert has_table  # the kernel's gated sweep always reads a table
         assert all(int(c) == 0 for k, c in enumerate(counts) if k not in (1 + g, 1 + 2 * R + g)), counts
         for t in terms[int(counts[1 + g]):]:
             assert t[0] == "linear" or t[3] == 0.0, t
