@@ -78,18 +78,17 @@ enum DevKind : int32_t {
                        // bytes, cm_reg bit 0: a 2^R table follows, cv_reg:
                        // active categories), then the term records by
                        // category, then the table
-    K_LAYER_SPLIT = 9, // uncontrolled gates diag(1, q) R diag(1, p), R real,
-                       // on the register bits of the mask (cm_reg): one
-                       // record per bit, lowest bit first, with R row-major
-                       // in m[0..3], p in m[4..5] and q in m[6..7]; cv_reg
-                       // bit b: bit b has a p, bit 8 + b: bit b has a q
+    K_LAYER_SPLIT = 9, // uncontrolled gates R diag(1, p), R real, on the
+                       // register bits of the mask (cm_reg): one record per
+                       // bit, lowest bit first, with R row-major in m[0..3]
+                       // and p in m[4..5]; cv_reg bit b: bit b has a p (a
+                       // gate's phase after R follows as a K_PHASE record)
     K_XSET = 10,       // X gates on register bits with at most one control, on
                        // a thread or non-tile bit: tpos entries of 4 bytes
                        // in m[] (target register bit, control kind
                        // XSET_CTRL_*, control bit, control value); each flips
                        // the thread's relabeling mask where its control holds
 };
-constexpr uint32_t SPLIT_POST_SHIFT = 8;
 constexpr int XSET_CTRL_NONE = 0, XSET_CTRL_THREAD = 2, XSET_CTRL_GLOBAL = 3;
 // entries of one K_XSET record: 4 bytes each in m[]
 template <typename Real>
@@ -279,8 +278,7 @@ struct Plan {
     bool chained = true;              // hgm_plan_opts.chained
     // The plan runs on the pass kernel's lean build: its phase blocks are all
     // compact terms, it has no controlled dense, real or anti-diagonal gate on
-    // a register bit, no split gate with a phase after its real gate and, in
-    // FP32, no complex layer (planner, lean_ops).
+    // a register bit and, in FP32, no complex layer (planner, lean_ops).
     bool lean = false;
     // Borrowers (requests of a server, hgm_server_submit_plan) hold a lease;
     // hgm_plan_free on a leased plan only marks it, and the last lease frees

@@ -572,17 +572,19 @@ __device__ __forceinline__ void reg_half_phase(A2 (&a)[1 << R], A2 f) {
 }
 
 // A split layer (K_LAYER_SPLIT): on each active register bit T the gate
-// diag(1, q) Rm diag(1, p), Rm real, as a phase on the registers whose bit T
-// is 1, the real gate (2 packed FP32 instructions per amplitude) and another
-// phase: 4-6 instructions per amplitude against the complex matrix's 8.
+// Rm diag(1, p), Rm real, as a phase on the registers whose bit T is 1 and the
+// real gate (2 packed FP32 instructions per amplitude): 4 instructions per
+// amplitude against the complex matrix's 8.  (A phase after the real part,
+// diag(1, q), follows the layer as a phase record: its code inside every
+// bit's body, never run by Rz.Ry gates, made layered passes 7% slower.)
 // Seen through a swapped label (xr bit T set) the gate is
-//   X diag(1, q) Rm diag(1, p) X = p q diag(1, q*) (X Rm X) diag(1, p*),
-// so the phases stay on the same registers, conjugated, the real matrix is
-// read bit-swapped and p q joins the thread's factor `pend`, which the layer
+//   X Rm diag(1, p) X = p (X Rm X) diag(1, p*),
+// so the phase stays on the same registers, conjugated, the real matrix is
+// read bit-swapped and p joins the thread's factor `pend`, which the layer
 // multiplies into all registers at its end.  Each active bit's record is
 // loaded while the previous bit's arithmetic runs (22-26 qubit FP32 layered
 // circuits: 7% faster than loading it where it is used).
-// one split-gate record as two 16-byte loads: (m00, m01, m10, m11), (p, q)
+// one split-gate record: (m00, m01, m10, m11) and p
 template <typename Real>
 struct SplitRec;
 template <>
@@ -593,20 +595,17 @@ struct SplitRec<float> {
         pq = __ldg(reinterpret_cast<const float4 *>(d->m) + 1);
     }
     __device__ __forceinline__ float2 p() const { return make_float2(pq.x, pq.y); }
-    __device__ __forceinline__ float2 q() const { return make_float2(pq.z, pq.w); }
 };
 template <>
 struct SplitRec<double> {
-    double2 r01, r23, pp, qq;
+    double2 r01, r23, pp;
     __device__ __forceinline__ void load(const DevOp<double> *__restrict__ d) {
         const double2 *m = reinterpret_cast<const double2 *>(d->m);
         r01 = __ldg(m);
         r23 = __ldg(m + 1);
         pp = __ldg(m + 2);
-        qq = __ldg(m + 3);
     }
     __device__ __forceinline__ double2 p() const { return pp; }
-    __device__ __forceinline__ double2 q() const { return qq; }
 };
 template <typename Real>
 __device__ __forceinline__ void split_real(const SplitRec<Real> &c, bool flip, Real (&mm)[8]);
@@ -625,7 +624,7 @@ __device__ __forceinline__ void split_real<double>(const SplitRec<double> &c, bo
     mm[6] = flip ? c.r01.x : c.r23.y;
 }
 
-template <typename Real, typename A2, int R, int T, bool LEAN>
+template <typename Real, typename A2, int R, int T>
 struct SplitStep {
     __device__ __forceinline__ static void run(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats,
                                                uint32_t mask, uint32_t phases, uint32_t xr, A2 &pend,
@@ -648,27 +647,18 @@ struct SplitStep {
                 split_real<Real>(c, flip, mm);
                 reg_real<Real, A2, R, T, false>(a, mm, 0u, 0u);
             }
-            // (the lean build has no post phases: apply_op, Plan::lean)
-            if (!LEAN && (phases & (1u << (SPLIT_POST_SHIFT + T)))) {
-                A2 q = c.q();
-                const A2 qf = cmul2<Real>(pend, q);
-                pend.x = flip ? qf.x : pend.x;
-                pend.y = flip ? qf.y : pend.y;
-                q.y = flip ? -q.y : q.y;
-                reg_half_phase<Real, A2, R, T>(a, q);
-            }
             mats++;
         }
-        SplitStep<Real, A2, R, T + 1, LEAN>::run(a, mats, mask, phases, xr, pend, cur);
+        SplitStep<Real, A2, R, T + 1>::run(a, mats, mask, phases, xr, pend, cur);
     }
 };
-template <typename Real, typename A2, int R, bool LEAN>
-struct SplitStep<Real, A2, R, R, LEAN> {
+template <typename Real, typename A2, int R>
+struct SplitStep<Real, A2, R, R> {
     __device__ __forceinline__ static void run(A2 (&)[1 << R], const DevOp<Real> *__restrict__, uint32_t, uint32_t,
                                                uint32_t, A2 &, SplitRec<Real> &) {}
 };
 
-template <typename Real, typename A2, int R, bool LEAN>
+template <typename Real, typename A2, int R>
 __device__ __forceinline__ void apply_split_layer(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ mats,
                                                   uint32_t mask, uint32_t phases, uint32_t xr) {
     A2 pend;
@@ -676,7 +666,7 @@ __device__ __forceinline__ void apply_split_layer(A2 (&a)[1 << R], const DevOp<R
     pend.y = 0;
     SplitRec<Real> cur;
     cur.load(mats);
-    SplitStep<Real, A2, R, 0, LEAN>::run(a, mats, mask, phases, xr, pend, cur);
+    SplitStep<Real, A2, R, 0>::run(a, mats, mask, phases, xr, pend, cur);
     // every thread of the warp reaches this point (ops are uniform)
     if (__any_sync(0xffffffffu, pend.x != (Real)1 || pend.y != (Real)0)) {
 #pragma unroll
@@ -1089,11 +1079,10 @@ __device__ __forceinline__ int op_records(const uint4 &hdr) {
 //
 // LEAN (Plan::lean): the build for plans whose phase blocks are all compact
 // terms, with no controlled dense, real or anti-diagonal gate on a register
-// bit, no split gate with a phase after its real gate and, in FP32, no
-// complex layer.  Leaving those bodies out of the kernel -- code the
-// benchmark circuits never run -- made 26-qubit FP32 layered passes 12% and
-// QFT passes 9% faster (fewer instruction-fetch stalls), so each plan runs
-// the smallest build it can.
+// bit and, in FP32, no complex layer.  Leaving those bodies out of the kernel
+// -- code the benchmark circuits never run -- made 26-qubit FP32 layered
+// passes 5% and QFT passes 9% faster (fewer instruction-fetch stalls), so
+// each plan runs the smallest build it can.
 template <typename Real, typename A2, int R, bool LEAN>
 __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__restrict__ op, const uint4 hdr,
                                          uint64_t base, uint32_t thr, uint32_t &xr) {
@@ -1126,7 +1115,7 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
         return;
     }
     if (kind == K_LAYER_SPLIT) {
-        apply_split_layer<Real, A2, R, LEAN>(a, op + 1, hdr.z, hdr.w, xr);
+        apply_split_layer<Real, A2, R>(a, op + 1, hdr.z, hdr.w, xr);
         return;
     }
     if (kind == K_LAYER || kind == K_LAYER_REAL) {

@@ -662,7 +662,6 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, const Roles 
                 for (int k = 0; k < R; k++) {
                     if (slot[k] < 0) continue;
                     if (pp[k] != 1.0) head.cv_reg |= 1u << k;
-                    if (qq[k] != 1.0) head.cv_reg |= 1u << (SPLIT_POST_SHIFT + k);
                 }
             }
             out.push_back(head);
@@ -677,6 +676,20 @@ void emit_phase(const std::vector<SOp> &ops, std::vector<int> rest, const Roles 
                     d.m[7] = (Real)qq[k].imag();
                     global *= sc[k];
                 }
+                out.push_back(d);
+            }
+            // a split gate's phase after its real part, diag(1, q), follows
+            // the layer as a phase record on the same register bit: the
+            // kernel's split layer carries only the phase before
+            for (int k = 0; k < R && all_split; k++) {
+                if (slot[k] < 0 || qq[k] == 1.0) continue;
+                DevOp<Real> d;
+                memset(&d, 0, sizeof d);
+                d.kind = K_PHASE;
+                d.tpos = d.tpos2 = k;
+                d.m[0] = (Real)1;
+                d.m[6] = (Real)qq[k].real();
+                d.m[7] = (Real)qq[k].imag();
                 out.push_back(d);
             }
             for (int idx : rest) {
@@ -733,8 +746,8 @@ struct OpList {
 
 // Whether the encoded op records need only the pass kernel's lean build
 // (Plan::lean): phase blocks of compact terms, layers (complex ones in FP64
-// only; split ones without a phase after the real gate), relabeling X
-// records, and on register bits only diagonal, phase and X gates.
+// only), relabeling X records, and on register bits only diagonal, phase and
+// X gates.
 template <typename Real>
 bool lean_ops(const std::vector<DevOp<Real>> &d, int R) {
     for (size_t i = 0; i < d.size();) {
@@ -748,11 +761,8 @@ bool lean_ops(const std::vector<DevOp<Real>> &d, int R) {
                 if (sizeof(Real) == 4) return false;
                 i += 1 + (size_t)__builtin_popcount(o.cm_reg);
                 break;
-            case K_LAYER_SPLIT:
-                if (o.cv_reg >> SPLIT_POST_SHIFT) return false;  // a phase after a real gate
-                i += 1 + (size_t)__builtin_popcount(o.cm_reg);
-                break;
             case K_LAYER_REAL:
+            case K_LAYER_SPLIT:
                 i += 1 + (size_t)__builtin_popcount(o.cm_reg);
                 break;
             case K_DENSE:

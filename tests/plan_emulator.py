@@ -38,7 +38,6 @@ SMALL_DT = {"<f8": np.dtype([("target", "<i4"), ("kind", "<i4"), ("cmask", "<u4"
 
 K_DENSE, K_REAL, K_DIAG, K_PHASE, K_ANTI, K_SWAP, K_LAYER, K_LAYER_REAL, K_PHASE_BLOCK, K_LAYER_SPLIT, K_XSET = range(11)
 XSET_CTRL_NONE, XSET_CTRL_THREAD, XSET_CTRL_GLOBAL = 0, 2, 3
-SPLIT_POST_SHIFT = 8
 PB_F_ACTIVE = 1 << 16
 REG_BITS = {"f64": 4, "f32": 5}
 PB_LINEAR = -2  # hgm_internal.h: a linear phase term
@@ -382,11 +381,10 @@ def run(plan, precision, state, iterations=1):
                                 continue
                             mm = recs[i + 1 + k]["m"].astype(np.float64)
                             if int(o["kind"]) == K_LAYER_SPLIT:
-                                # diag(1, q) Rm diag(1, p): Rm real in m[0..3], p in m[4..5], q in m[6..7]
+                                # Rm diag(1, p): Rm real in m[0..3], p in m[4..5]
                                 flags = int(o["cv_reg"])
                                 p = mm[4] + 1j * mm[5] if (flags >> t) & 1 else 1.0
-                                q = mm[6] + 1j * mm[7] if (flags >> (SPLIT_POST_SHIFT + t)) & 1 else 1.0
-                                mm = np.array([mm[0], mm[1] * p, mm[2] * q, mm[3] * q * p], dtype=np.complex128)
+                                mm = np.array([mm[0], mm[1] * p, mm[2], mm[3] * p], dtype=np.complex128)
                             else:
                                 mm = mm[0::2] + 1j * mm[1::2]
                             tile = apply_reg_pair(tile, lay, R, W, lane, warp, reg, t, np.ones(T, bool),

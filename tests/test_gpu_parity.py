@@ -162,8 +162,8 @@ def zyz_layered(n, layers, seed):
 
 @pytest.mark.parametrize("n,warp_bits", [(14, 2), (18, 3)])
 def test_split_layers_post_phase(sq, n, warp_bits):
-    """Split gates with a phase after the real part too (Rz.Ry.Rz), which only
-    the kernels' full build carries: FP32 against the FP64 oracle."""
+    """Split gates with a phase after the real part too (Rz.Ry.Rz; that phase
+    follows the split layer as a phase record): FP32 against the FP64 oracle."""
     spec = zyz_layered(n, 4, seed=n)
     want = oracle_state(spec, "f64")
     got, _ = engine_state(sq, spec, "f32", warp_bits=warp_bits, renorm_every=0)
