@@ -101,12 +101,12 @@ typedef struct hgm_plan_opts {
     int renorm_every;/* FP32: rescale to unit norm every k passes (0 = never) */
     int chained;     /* 1 (default): a state of at most 32 MiB runs all its passes
                         in one persistent launch; 0: one launch per pass */
-    int split_layers;/* 1 (FP32 default): an uncontrolled dense gate of a
-                        layer whose matrix is s diag(1,q) R diag(1,p) with R
-                        real and |s| = |p| = |q| = 1 (every unitary is) runs as
-                        phase, real gate, phase, and the scalars s of all such
-                        gates are applied once at the end of the plan; 0 (FP64
-                        default): every dense gate runs as a complex matrix */
+    int split_layers;/* 1 (default): an uncontrolled dense gate of a layer
+                        whose matrix is s diag(1,q) R diag(1,p) with R real and
+                        |s| = |p| = |q| = 1 (every unitary is) runs as phase,
+                        real gate, phase, and the scalars s of all such gates
+                        are applied once at the end of the plan; 0: every dense
+                        gate runs as a complex matrix */
     int reg_bits;    /* amplitudes a thread keeps in registers = 2^reg_bits:
                         FP64 4; FP32 4 or 5; -1 = default (FP64 4, FP32 5) */
 } hgm_plan_opts;
