@@ -278,7 +278,7 @@ struct Plan {
     bool chained = true;              // hgm_plan_opts.chained
     // The plan runs on the pass kernel's lean build: its phase blocks are all
     // compact terms, it has no controlled dense, real or anti-diagonal gate on
-    // a register bit and, in FP32, no complex layer (planner, lean_ops).
+    // a register bit and no complex layer (planner, lean_ops).
     bool lean = false;
     // Borrowers (requests of a server, hgm_server_submit_plan) hold a lease;
     // hgm_plan_free on a leased plan only marks it, and the last lease frees

@@ -1079,7 +1079,7 @@ __device__ __forceinline__ int op_records(const uint4 &hdr) {
 //
 // LEAN (Plan::lean): the build for plans whose phase blocks are all compact
 // terms, with no controlled dense, real or anti-diagonal gate on a register
-// bit and, in FP32, no complex layer.  Leaving those bodies out of the kernel
+// bit and no complex layer.  Leaving those bodies out of the kernel
 // -- code the benchmark circuits never run -- made 26-qubit FP32 layered
 // passes 5% and QFT passes 9% faster (fewer instruction-fetch stalls), so
 // each plan runs the smallest build it can.
@@ -1121,7 +1121,7 @@ __device__ __forceinline__ void apply_op(A2 (&a)[1 << R], const DevOp<Real> *__r
     if (kind == K_LAYER || kind == K_LAYER_REAL) {
         const uint32_t mask = hdr.z;  // active register bits
         if (kind == K_LAYER) {
-            if constexpr (!LEAN || sizeof(Real) == 8) apply_layer<Real, A2, R, false>(a, op + 1, mask, xr);
+            if constexpr (!LEAN) apply_layer<Real, A2, R, false>(a, op + 1, mask, xr);
         } else {
             apply_layer<Real, A2, R, true>(a, op + 1, mask, xr);
         }

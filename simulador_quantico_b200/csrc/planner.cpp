@@ -745,9 +745,9 @@ struct OpList {
 };
 
 // Whether the encoded op records need only the pass kernel's lean build
-// (Plan::lean): phase blocks of compact terms, layers (complex ones in FP64
-// only), relabeling X records, and on register bits only diagonal, phase and
-// X gates.
+// (Plan::lean): phase blocks of compact terms, real and split layers,
+// relabeling X records, and on register bits only diagonal, phase and X
+// gates.
 template <typename Real>
 bool lean_ops(const std::vector<DevOp<Real>> &d, int R) {
     for (size_t i = 0; i < d.size();) {
@@ -758,9 +758,7 @@ bool lean_ops(const std::vector<DevOp<Real>> &d, int R) {
                 i += 1 + (size_t)o.tpos;
                 break;
             case K_LAYER:
-                if (sizeof(Real) == 4) return false;
-                i += 1 + (size_t)__builtin_popcount(o.cm_reg);
-                break;
+                return false;
             case K_LAYER_REAL:
             case K_LAYER_SPLIT:
                 i += 1 + (size_t)__builtin_popcount(o.cm_reg);
