@@ -276,6 +276,11 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
     A2 *sm = reinterpret_cast<A2 *>(smem_raw);
     __shared__ long long s_item;
     __shared__ int s_skip;
+    // the item's pass arguments, copied once per item: the tile code reads
+    // them many times (the tile-bit map byte by byte), from shared memory
+    // rather than through L1
+    __shared__ __align__(16) PassArgs s_pa;
+    static_assert(sizeof(PassArgs) % 4 == 0, "PassArgs copies as words");
     const long long seq = total >> tile_bits;  // passes in the sequence
     for (;;) {
         if (threadIdx.x == 0) {
@@ -315,8 +320,14 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
                     scale_in = norms + (g / renorm - 1) % CHAIN_NORM_SLOTS;
                 }
             }
-            run_tile<Real, R, W, LEAN>(state, passes[g % npasses], (uint64_t)(it & ((1ll << tile_bits) - 1)), sm, flags,
-                                 norm_out, scale_in);
+            {
+                const uint32_t *src = reinterpret_cast<const uint32_t *>(passes + g % npasses);
+                uint32_t *dst = reinterpret_cast<uint32_t *>(&s_pa);
+                for (int w = threadIdx.x; w < (int)(sizeof(PassArgs) / 4); w += blockDim.x) dst[w] = __ldg(src + w);
+            }
+            __syncthreads();
+            run_tile<Real, R, W, LEAN>(state, s_pa, (uint64_t)(it & ((1ll << tile_bits) - 1)), sm, flags, norm_out,
+                                       scale_in);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
