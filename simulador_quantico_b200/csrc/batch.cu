@@ -96,6 +96,9 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
     __shared__ long long s_item;
     __shared__ int s_task;
     __shared__ int s_skip;
+    // the item's pass arguments, copied once per item into shared memory (the
+    // tile code reads them many times; chained kernel, kernels.cu)
+    __shared__ __align__(16) PassArgs s_pa;
     for (;;) {
         if (threadIdx.x == 0) {
             const long long it = (long long)atomicAdd(next_item, 1ull);
@@ -134,7 +137,11 @@ __global__ void __launch_bounds__(32 << W) __maxnreg__((pass_max_regs<Real, R>()
                 small_task<Real>(reinterpret_cast<A2 *>(t.state), t.n,
                                  reinterpret_cast<const SmallOp<Real> *>(t.small_ops), t.n_small_ops, sm);
             } else {
-                run_tile<Real, R, W>(reinterpret_cast<A2 *>(t.state), t.pa, (uint64_t)(it - t.tile_begin), sm);
+                const uint32_t *src = reinterpret_cast<const uint32_t *>(&t.pa);
+                uint32_t *dst = reinterpret_cast<uint32_t *>(&s_pa);
+                for (int w = threadIdx.x; w < (int)(sizeof(PassArgs) / 4); w += blockDim.x) dst[w] = __ldg(src + w);
+                __syncthreads();
+                run_tile<Real, R, W>(reinterpret_cast<A2 *>(t.state), s_pa, (uint64_t)(it - t.tile_begin), sm);
             }
         }
         __syncthreads();
